@@ -1,0 +1,321 @@
+"""Benchmark: amplitude updates per second of the B200 CUDAEngine.
+
+Workload (one GPU): the 30-qubit complex64 (8.6 GB) random circuit of depth
+24 -- per layer RX/RY/RZ(theta~U[0,2pi)) on every qubit plus CZ on seeded
+random disjoint pairs (1080 gates) -- run through the tiled engine.  A step =
+one execution of the compiled circuit on a state already resident in HBM
+(reset to |0...0> between steps, untimed, like the reference benchmark loop,
+bench_hw_awareness.cpp:102-107).  amp-updates = gates x 2^n (pre-fusion
+gates, so fusion and tiling count as speed).
+
+  python bench.py [--gpus N --steps K --warmup W]      our engine (N replicas)
+  python bench.py --impl reference                     the reference CPU engine
+
+Under torchrun each rank runs an independent replica on its own GPU (the
+path does not shard: "replicas only"); `value` is the sum over ranks of
+amp-updates divided by the max-over-ranks device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "amp-updates/s"
+UNIT = "amp-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--qubits", type=int, default=30)
+    ap.add_argument("--depth", type=int, default=24)
+    ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--mode", default="tiled")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    return ap.parse_args()
+
+
+def workload(args):
+    from qlassical_b200 import circuits
+    return circuits.random_rot_cz(args.qubits, args.depth, seed=args.seed)
+
+
+def config_of(args, module, extra=None):
+    c = {
+        "workload": f"random RX/RY/RZ + CZ-pairs circuit, {args.qubits} qubits, depth {args.depth}",
+        "n_qubits": args.qubits,
+        "depth": args.depth,
+        "seed": args.seed,
+        "gates": module.gate_count(),
+        "state_bytes": (1 << args.qubits) * 8,
+        "l2": "state (complex64) larger than the 126 MB L2; no flush needed",
+    }
+    if extra:
+        c.update(extra)
+    return c
+
+
+class ClockSampler:
+    """nvidia-smi clocks sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except OSError:
+            rows = []
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(args, module, max_gates):
+    """The reference CPUOpenMPEngine (oracle/_ref, its Release flags) on the
+    first `max_gates` instructions of the same circuit at the same size."""
+    from oracle import oracle
+    from qlassical_b200 import circuits
+    from qlassical_b200.ir import IRModule
+    ref = circuits.to_reference_ir(module)
+    sample = IRModule(module.num_qubits, unitary_pool=ref.unitaries())
+    sample.set_program(ref.program()[:max_gates])
+    t = oracle.time_reference(sample, reps=1)
+    value = max_gates * float(1 << module.num_qubits) / t
+    return {"value": value, "unit": UNIT, "cores": oracle.reference_threads(), "kind": "reference",
+            "sample": f"first {max_gates} of {module.gate_count()} gates of the same {module.num_qubits}-qubit "
+                      f"circuit (CZ as 2-qubit UNITARY), complex128, {t:.2f} s"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_PROC_BIND", "true")
+    os.environ.setdefault("OMP_PLACES", "cores")
+    module = workload(args)
+    from oracle import oracle
+    from qlassical_b200 import circuits
+    from qlassical_b200.ir import IRModule
+    if not oracle.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference sources absent)"}))
+        return
+    ref = circuits.to_reference_ir(module)
+    gates = 15
+    sample = IRModule(module.num_qubits, unitary_pool=ref.unitaries())
+    sample.set_program(ref.program()[:gates])
+    for _ in range(args.warmup):
+        oracle.time_reference(sample, reps=1)
+    times = [oracle.time_reference(sample, reps=1) for _ in range(args.steps)]
+    total = sum(times)
+    value = args.steps * gates * float(1 << module.num_qubits) / total
+    cores = oracle.reference_threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic", "config": config_of(args, module, {"sample_gates_per_step": gates}),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"first {gates} gates of the circuit per step, complex128, CPUOpenMPEngine"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from __graft_entry__ import package
+    q = package()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    q.engine.set_device(local)
+
+    module = workload(args)
+    n = module.num_qubits
+    gates = module.gate_count()
+    eng = q.CUDAEngine(n, seed=1, mode=args.mode)
+    plan = eng.compile(module)
+    pstats = plan.stats()
+    stream = torch.cuda.ExternalStream(eng.stream())
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        eng.reset()
+        eng.run(plan)
+    eng.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            eng.reset()
+            starts[i].record(stream)
+            eng.run(plan)
+            ends[i].record(stream)
+        eng.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    clocks = clk.summary()
+
+    amp_updates_step = gates * float(1 << n)
+    value = world * args.steps * amp_updates_step / (total_ms / 1e3)
+    passes = pstats["sweeps"]
+    avg_launch_ms = (total_ms / args.steps) / max(1, pstats["launches"])
+    bytes_per_launch = 16.0 * float(1 << n)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = bytes_per_launch / (avg_launch_ms / 1e3) / 1e9
+    hbm_gbs = passes * bytes_per_launch / ((total_ms / args.steps) / 1e3) / 1e9
+
+    # e2e: the public call with host buffers: execute(program, pool) uploads
+    # the instruction stream + pool, runs, then <Z_i> comes back to the host.
+    prog = module.program()
+    pool = module.unitaries()
+    h2d = prog.nbytes + pool.data.nbytes + pool.metadata().nbytes
+    d2h = 8 * n
+    e2e_times = []
+    for _ in range(max(1, min(args.steps, 3))):
+        eng.reset()
+        eng.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        eng.execute(prog, pool)
+        ez = eng.expect_z()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_t = statistics.mean(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_t], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+    e2e_value = world * amp_updates_step / e2e_t
+
+    extra = {"mode": args.mode, "passes_per_step": passes, "launches_per_step": pstats["launches"],
+             "parallelism": f"replicas x{world}"}
+    plain = None
+    if not args.no_plain and rank == 0:
+        eng.reset()
+        eng.set_mode("plain")
+        pplan = eng.compile(module)
+        eng.reset()
+        eng.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        eng.run(pplan)
+        e.record(stream)
+        eng.synchronize()
+        pms = s.elapsed_time(e)
+        pst = pplan.stats()
+        plain = {"value": amp_updates_step / (pms / 1e3), "ms": pms, "sweeps": pst["sweeps"],
+                 "hbm_gbs": pst["sweeps"] * bytes_per_launch / (pms / 1e3) / 1e9}
+        eng.set_mode(args.mode)
+        del pplan
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32)", "data": "synthetic",
+        "config": config_of(args, module, extra),
+        "hbm_gbs": hbm_gbs,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "k_tile_pass", "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"},
+        "clocks": clocks,
+        "gpu_launches": args.steps * pstats["launches"],
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+    }
+    if plain:
+        line["plain_gpu"] = plain
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(args, module, max_gates=45)
+        except Exception as ex:  # the oracle libraries are test infrastructure
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
+                                    "sample": f"unavailable: {ex}"}
+    if rank == 0:
+        print(json.dumps(line))
+    del plan
+    del eng
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,232 @@
+/*
+ * qlassical_b200.h -- C ABI of the B200 execution backend for Qlassical.
+ *
+ * This is the drop-in boundary: the reference simulator's hot path is
+ * CPUOpenMPEngine::execute over a transpiled IRModule
+ * (include/backend/cpu_openmp_engine.hpp:143-225).  Every entry point below
+ * replaces one member of the reference's ExecutionEngine / StateVector /
+ * Middleware interfaces (cited per function) and takes only plain pointers,
+ * sizes and opaque handles, so a C++20 wrapper (include/qlassical_b200/
+ * cuda_engine.hpp), a ctypes binding or any other FFI can sit on top of it.
+ *
+ * Conventions (identical to the reference):
+ *   - qubit q <-> bit q of the amplitude index (little endian);
+ *   - dense matrices are row-major, matrix-index bit i <-> instr.qubits[i]
+ *     (cpu_openmp_engine.hpp:558-566);
+ *   - host amplitudes are interleaved complex128 (std::complex<double>),
+ *     device amplitudes are complex64 (float2), 256-byte aligned.
+ *
+ * Every function returns a qlb_status.  No C++ exception crosses the ABI;
+ * qlb_last_error() returns a thread-local message for the last failure.
+ */
+#ifndef QLASSICAL_B200_H
+#define QLASSICAL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Wire format                                                              */
+/* ------------------------------------------------------------------------ */
+
+/* Gate type codes: the values of qlassical::GateType (frontend.hpp:26-51),
+ * plus two additive diagonal types (CZ, CP) in the free two-qubit range. */
+enum qlb_gate_type {
+    QLB_H = 0x00, QLB_X = 0x01, QLB_Y = 0x02, QLB_Z = 0x03, QLB_S = 0x04,
+    QLB_RX = 0x10, QLB_RY = 0x11, QLB_RZ = 0x12,
+    QLB_CX = 0x20, QLB_SWAP = 0x21,
+    QLB_CZ = 0x22,          /* additive: diag(1,1,1,-1) on (qubits[0], qubits[1]) */
+    QLB_CP = 0x23,          /* additive: diag(1,1,1,e^{i*param}) */
+    QLB_CCX = 0x30, QLB_CSWAP = 0x31,
+    QLB_UNITARY = 0x80,
+    QLB_FUSED_BLOCK = 0xE0, QLB_GLOBAL_SWAP = 0xE1,
+    QLB_BARRIER = 0xF0, QLB_MEASURE = 0xF1
+};
+
+/* Byte-for-byte the layout of qlassical::GateInstr (frontend.hpp:84-105):
+ * offsets 0/1/2/8/12, 16 bytes, 16-byte aligned.  The reference's two pad
+ * bytes (offset 6-7) carry qubits 4 and 5 of a 5- or 6-qubit FUSED_BLOCK or
+ * UNITARY; they stay 0 for every other instruction, which the reference
+ * ignores, so streams remain readable by the reference engine. */
+typedef struct qlb_gate_instr {
+    uint8_t type;
+    uint8_t flags_arity;       /* low nibble: arity, high nibble: flags */
+    uint8_t qubits[4];
+    uint8_t qubits_ext[2];     /* reference: uint16_t _pad */
+    union { float param; uint32_t matrix_idx; } payload;
+    uint32_t uid;
+} qlb_gate_instr;
+
+/* UnitaryPool::MatrixEntry (frontend.hpp:118-123): 12 bytes. */
+typedef struct qlb_matrix_entry {
+    uint32_t offset;           /* start index (in complex elements) into data */
+    uint32_t num_elements;     /* 4^k */
+    uint8_t  num_qubits;       /* k */
+    uint8_t  pad[3];
+} qlb_matrix_entry;
+
+/* A read-only view of a UnitaryPool (frontend.hpp:117-164):
+ * data = interleaved complex128, 2*num_elements doubles. */
+typedef struct qlb_pool_view {
+    const double*           data;
+    uint64_t                num_elements;
+    const qlb_matrix_entry* metadata;
+    uint64_t                num_matrices;
+} qlb_pool_view;
+
+/* ------------------------------------------------------------------------ */
+/* Status                                                                   */
+/* ------------------------------------------------------------------------ */
+
+typedef enum qlb_status {
+    QLB_OK = 0,
+    QLB_ERR_INVALID_ARG = 1,   /* -> std::invalid_argument */
+    QLB_ERR_OOM = 2,           /* -> std::bad_alloc */
+    QLB_ERR_CUDA = 3,          /* -> std::runtime_error */
+    QLB_ERR_UNKNOWN_GATE = 4,  /* -> std::runtime_error (cpu_openmp_engine.hpp:221-222) */
+    QLB_ERR_NOT_NORMALIZED = 5,/* -> std::invalid_argument (cpu_state_vector.hpp:97-106) */
+    QLB_ERR_TIMEOUT = 6,       /* a bounded device wait gave up */
+    QLB_ERR_STATE = 7          /* call order violated (e.g. empty state) */
+} qlb_status;
+
+const char* qlb_last_error(void);
+/* Library version string and the CUDA device it will use. */
+const char* qlb_version(void);
+/* Selects the CUDA device used by later calls from this thread (the library
+ * links its own CUDA runtime, so a host framework's current device is not
+ * inherited). */
+int qlb_set_device(int device);
+int qlb_device_info(int* sm_count, uint64_t* free_bytes, uint64_t* total_bytes);
+
+/* ------------------------------------------------------------------------ */
+/* CUDAStateVector (replaces CPUStateVector, cpu_state_vector.hpp:24-162)   */
+/* ------------------------------------------------------------------------ */
+
+typedef struct qlb_state* qlb_state_t;
+
+int qlb_state_create(qlb_state_t* out);                                  /* CPUStateVector() */
+int qlb_state_destroy(qlb_state_t sv);
+int qlb_state_initialize(qlb_state_t sv, uint32_t num_qubits);           /* :54-78  */
+int qlb_state_initialize_from(qlb_state_t sv, const double* amps_c128,
+                              uint64_t dim);                             /* :82-115 */
+int qlb_state_num_qubits(qlb_state_t sv, uint32_t* out);                 /* :148-150 */
+int qlb_state_dimension(qlb_state_t sv, uint64_t* out);                  /* :152-154 */
+int qlb_state_empty(qlb_state_t sv, int* out);                           /* :156-158 */
+int qlb_state_download(qlb_state_t sv, double* out_c128, uint64_t dim);  /* amplitudes() */
+int qlb_state_device_ptr(qlb_state_t sv, void** out_float2);             /* data() */
+
+/* ------------------------------------------------------------------------ */
+/* CUDAEngine (replaces CPUOpenMPEngine, cpu_openmp_engine.hpp:51-672)      */
+/* ------------------------------------------------------------------------ */
+
+typedef struct qlb_engine* qlb_engine_t;
+
+/* Execution strategies for execute():
+ *  PLAIN    - one HBM sweep per instruction (the plain GPU path);
+ *  TILED    - runs of instructions applied inside shared-memory tiles,
+ *             dense blocks on FP32 CUDA cores;
+ *  TILED_TC - as TILED, dense blocks of >= 4 qubits on the tensor cores
+ *             (tcgen05, split-precision bf16, FP32 accumulate). */
+enum qlb_exec_mode { QLB_MODE_PLAIN = 0, QLB_MODE_TILED = 1, QLB_MODE_TILED_TC = 2 };
+
+int qlb_engine_create(qlb_engine_t* out, uint32_t num_qubits, int has_seed,
+                      uint64_t seed, uint64_t reserve_meas);             /* :65-80   */
+int qlb_engine_create_from_amplitudes(qlb_engine_t* out, const double* amps_c128,
+                      uint64_t dim, int has_seed, uint64_t seed,
+                      uint64_t reserve_meas);                            /* :87-102  */
+int qlb_engine_create_from_state(qlb_engine_t* out, qlb_state_t sv);     /* :105-107 (moves sv) */
+int qlb_engine_destroy(qlb_engine_t e);
+int qlb_engine_set_state_vector(qlb_engine_t e, qlb_state_t sv);         /* :110-112 (moves sv) */
+int qlb_engine_extract_state_vector(qlb_engine_t e, qlb_state_t out_sv); /* :245-247 (moves into out_sv) */
+int qlb_engine_reset(qlb_engine_t e);                                    /* :119-122 */
+int qlb_engine_reset_to(qlb_engine_t e, const double* amps_c128, uint64_t dim); /* :125-128 */
+int qlb_engine_set_seed(qlb_engine_t e, uint64_t seed);                  /* :130-132 */
+int qlb_engine_reserve_measurements(qlb_engine_t e, uint64_t count);     /* :134-136 */
+int qlb_engine_measurements(qlb_engine_t e, const uint8_t** data, uint64_t* count); /* :138-140 */
+int qlb_engine_execute(qlb_engine_t e, const qlb_gate_instr* program,
+                       uint64_t count, const qlb_pool_view* pool);       /* :143-225 */
+int qlb_engine_state(qlb_engine_t e, double* out_c128, uint64_t dim);    /* :231-233 (D2H + widen) */
+int qlb_engine_num_qubits(qlb_engine_t e, uint32_t* out);                /* :235-237 */
+int qlb_engine_set_mode(qlb_engine_t e, int mode);
+int qlb_engine_get_mode(qlb_engine_t e, int* mode);
+/* Engine options.  QLB_OPT_PHYSICAL_GLOBAL_SWAP = 1 makes GLOBAL_SWAP move
+ * data (one bandwidth-bound swap pass each, logical order restored when
+ * execute() returns); 0 (default) applies the permutation lazily by
+ * re-addressing later instructions, which gives the same state with no
+ * data movement. */
+enum qlb_option { QLB_OPT_PHYSICAL_GLOBAL_SWAP = 1 };
+int qlb_engine_set_option(qlb_engine_t e, int key, int64_t value);
+int qlb_engine_synchronize(qlb_engine_t e);
+/* The device state pointer (float2 *) and the stream the engine launches on. */
+int qlb_engine_device_state(qlb_engine_t e, void** out_float2);
+int qlb_engine_stream(qlb_engine_t e, void** out_cuda_stream);
+/* Statistics of the last execute(): HBM sweeps, kernel launches, tile passes. */
+typedef struct qlb_exec_stats {
+    uint64_t instructions;      /* instructions in the program */
+    uint64_t sweeps;            /* full-state HBM read+write passes executed */
+    uint64_t launches;          /* kernels launched */
+    uint64_t tile_passes;       /* tiled passes (subset of sweeps) */
+    uint64_t permute_passes;    /* qubit-permutation passes (subset of sweeps) */
+    uint64_t dense_ops;         /* dense unitaries applied */
+    uint64_t tc_ops;            /* dense unitaries applied on the tensor cores */
+    double   sweep_bytes;       /* algorithmic bytes: 16 B/amp per full sweep */
+} qlb_exec_stats;
+int qlb_engine_last_stats(qlb_engine_t e, qlb_exec_stats* out);
+
+/* Compiled programs.  execute() == compile + run + destroy.  A plan holds the
+ * engine-ready form of one program (its pass schedule and every operand
+ * already in device memory) for one qubit count and execution mode, so it
+ * can be run many times with no host work besides the launches.  Running a
+ * plan whose qubit count differs from the engine's state is an error. */
+typedef struct qlb_plan* qlb_plan_t;
+int qlb_engine_compile(qlb_engine_t e, const qlb_gate_instr* program, uint64_t count,
+                       const qlb_pool_view* pool, qlb_plan_t* out);
+int qlb_engine_run(qlb_engine_t e, qlb_plan_t plan);
+int qlb_plan_stats(qlb_plan_t plan, qlb_exec_stats* out);
+int qlb_plan_destroy(qlb_plan_t plan);
+
+/* FP64 reductions over the device state (no reference counterpart except
+ * the probability reduction inside apply_measure, :622-630). */
+int qlb_engine_norm_sq(qlb_engine_t e, double* out);
+int qlb_engine_prob_one(qlb_engine_t e, uint32_t qubit, double* out);
+int qlb_engine_expect_z(qlb_engine_t e, double* out, uint32_t num_qubits);
+/* Draws `shots` basis states from |amp|^2 with a counter-based generator
+ * keyed by `seed`; identical seeds give identical samples on any launch. */
+int qlb_engine_sample(qlb_engine_t e, uint64_t seed, uint64_t shots, uint64_t* out);
+
+/* ------------------------------------------------------------------------ */
+/* GPU middle end (replaces Middleware::transpile_gpu, middleware.hpp:866)  */
+/* ------------------------------------------------------------------------ */
+
+typedef struct qlb_transpile_config {
+    int      enable_gate_fusion;   /* TranspilerConfig::enable_gate_fusion (:363) */
+    int      enable_hw_awareness;  /* TranspilerConfig::enable_hw_awareness (:364) */
+    int      cost_model_type;      /* 0 THRESHOLD, 1 GREEDY (:352-356) */
+    uint32_t numa_penalty;         /* (:370) */
+    uint32_t swap_penalty;         /* (:371) */
+    int      k_safe;               /* <0: from the GPU topology (shared-memory window) */
+    int      max_fusion_qubits;    /* 1..6; the reference's limit is 4 (:137) */
+    int      reference_fusable_set;/* 1: only H,X,Y,Z,S,CX,UNITARY,FUSED_BLOCK fuse (:442-448) */
+} qlb_transpile_config;
+
+typedef struct qlb_module* qlb_module_t;
+
+void qlb_transpile_config_default(qlb_transpile_config* cfg);
+int qlb_transpile_gpu(const qlb_gate_instr* program, uint64_t count,
+                      const qlb_pool_view* pool, uint32_t num_qubits,
+                      const qlb_transpile_config* cfg, qlb_module_t* out);
+int qlb_module_destroy(qlb_module_t m);
+int qlb_module_program(qlb_module_t m, const qlb_gate_instr** program, uint64_t* count);
+int qlb_module_pool(qlb_module_t m, qlb_pool_view* out);
+/* GPUTopology::get_safe_qubit_limit(): the shared-memory tile window. */
+int qlb_gpu_safe_qubit_limit(uint32_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QLASSICAL_B200_H */

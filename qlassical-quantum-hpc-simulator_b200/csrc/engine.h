@@ -1,0 +1,69 @@
+// engine.h -- C++ engine objects behind the C ABI (qlassical_b200.h).
+#pragma once
+
+#include <array>
+#include <cstdint>
+#include <random>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/qlassical_b200.h"
+
+struct qlb_state {
+    float2* d = nullptr;   // 2^n complex64 amplitudes (cudaMalloc, 256-B aligned)
+    uint32_t n = 0;
+    uint64_t dim = 0;      // 0 <=> empty
+};
+
+namespace qlb {
+
+// Error carrier used inside the library; converted to a status at the ABI.
+struct Error {
+    qlb_status code;
+    std::string msg;
+};
+
+[[noreturn]] void fail(qlb_status code, const std::string& msg);
+void check_cuda(cudaError_t e, const char* what);
+
+// Grow-only device / pinned host buffers.
+struct DeviceBuffer {
+    void* p = nullptr;
+    size_t cap = 0;
+    void* ensure(size_t bytes);
+    void release();
+    ~DeviceBuffer() { release(); }
+};
+struct PinnedBuffer {
+    void* p = nullptr;
+    size_t cap = 0;
+    void* ensure(size_t bytes);
+    void release();
+    ~PinnedBuffer() { release(); }
+};
+
+void state_allocate(qlb_state& sv, uint32_t n);   // throws OOM
+void state_free(qlb_state& sv);
+// Uploads complex128 host amplitudes into sv (allocated), via device staging.
+void state_upload_c128(qlb_state& sv, const double* amps, uint64_t dim, cudaStream_t s, DeviceBuffer& staging);
+void state_download_c128(const qlb_state& sv, double* out, cudaStream_t s, DeviceBuffer& staging);
+
+struct TilePlanner;  // tile.cpp
+
+}  // namespace qlb
+
+struct qlb_engine {
+    qlb_state sv;
+    cudaStream_t stream = nullptr;
+    std::mt19937_64 rng;                                  // cpu_openmp_engine.hpp:252
+    std::uniform_real_distribution<double> dist{0.0, 1.0};  // :253
+    std::vector<uint8_t> measurements;
+    int mode = QLB_MODE_TILED;
+    int physical_global_swap = 0;   // execute GLOBAL_SWAP as a data permutation
+    qlb::DeviceBuffer red_partial, red_out, staging;
+    qlb::PinnedBuffer host_pinned, host_prog;
+    qlb_exec_stats stats{};
+    std::vector<double> last_marginals;
+};

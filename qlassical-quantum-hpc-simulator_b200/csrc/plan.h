@@ -1,0 +1,42 @@
+// plan.h -- a compiled program (qlb_plan): the step list of one execute()
+// with every operand already in device memory.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "engine.h"
+#include "tile.h"
+
+namespace qlb {
+
+enum StepKind : uint8_t {
+    STEP_PASS = 0,      // one tile-kernel launch (index = pass)
+    STEP_PLAIN = 1,     // one plain instruction (instr, memory qubits)
+    STEP_MEASURE = 2,   // MEASURE of memory qubit `instr.qubits[0]`
+    STEP_SWAP = 3       // exchange of memory qubits instr.qubits[0..1] (data moves)
+};
+
+struct PlanStep {
+    uint8_t kind;
+    uint32_t index;
+    qlb_gate_instr instr;
+    uint64_t mat_off;   // float2 offset of a dense matrix in the plan's device buffer
+};
+
+}  // namespace qlb
+
+struct qlb_plan {
+    uint32_t n = 0;
+    int mode = 0;
+    std::vector<qlb::PlanStep> steps;
+    qlb::DeviceBuffer dev;   // [passes | phases | ops | phase words | tile mats | plain mats]
+    size_t o_pass = 0, o_phase = 0, o_ops = 0, o_pd = 0, o_mat = 0, o_plain = 0;
+    qlb_exec_stats stats{};
+};
+
+namespace qlb {
+// Builds a plan for the engine's qubit count, mode and options.
+qlb_plan* compile_plan(qlb_engine& e, const qlb_gate_instr* prog, uint64_t count, const qlb_pool_view* pool);
+void run_plan(qlb_engine& e, const qlb_plan& p);
+}  // namespace qlb
