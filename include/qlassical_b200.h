@@ -202,15 +202,24 @@ int qlb_engine_sample(qlb_engine_t e, uint64_t seed, uint64_t shots, uint64_t* o
 /* GPU middle end (replaces Middleware::transpile_gpu, middleware.hpp:866)  */
 /* ------------------------------------------------------------------------ */
 
+/* WindowingCostModel::evaluate_swap (middleware.hpp:50-53) as a C callback:
+ * return 1 and fill (*active, *victim) -- logical qubits -- to request a
+ * swap, 0 for none. */
+typedef int (*qlb_cost_model_fn)(void* ctx, const uint32_t* window_frequencies,
+                                 const uint16_t* log_to_phys, const uint16_t* phys_to_log,
+                                 uint32_t num_qubits, uint16_t* active, uint16_t* victim);
+
 typedef struct qlb_transpile_config {
     int      enable_gate_fusion;   /* TranspilerConfig::enable_gate_fusion (:363) */
     int      enable_hw_awareness;  /* TranspilerConfig::enable_hw_awareness (:364) */
-    int      cost_model_type;      /* 0 THRESHOLD, 1 GREEDY (:352-356) */
+    int      cost_model_type;      /* 0 THRESHOLD, 1 GREEDY, 2 CUSTOM (:352-356) */
     uint32_t numa_penalty;         /* (:370) */
     uint32_t swap_penalty;         /* (:371) */
-    int      k_safe;               /* <0: from the GPU topology (shared-memory window) */
+    int      k_safe;               /* <0: from the GPU topology (the tile window) */
     int      max_fusion_qubits;    /* 1..6; the reference's limit is 4 (:137) */
     int      reference_fusable_set;/* 1: only H,X,Y,Z,S,CX,UNITARY,FUSED_BLOCK fuse (:442-448) */
+    qlb_cost_model_fn custom_cost_model;   /* TranspilerConfig::custom_cost_model (:379) */
+    void*    custom_cost_model_ctx;
 } qlb_transpile_config;
 
 typedef struct qlb_module* qlb_module_t;

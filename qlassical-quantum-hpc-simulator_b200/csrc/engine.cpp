@@ -48,6 +48,7 @@ int sm_count() {
 }
 
 void fail(qlb_status code, const std::string& msg) { throw Error{code, msg}; }
+void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 void check_cuda(cudaError_t e, const char* what) {
     if (e == cudaSuccess) return;

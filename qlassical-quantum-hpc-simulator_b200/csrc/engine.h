@@ -27,6 +27,7 @@ struct Error {
 
 [[noreturn]] void fail(qlb_status code, const std::string& msg);
 void check_cuda(cudaError_t e, const char* what);
+void set_last_error(const std::string& msg);
 
 // Grow-only device / pinned host buffers.
 struct DeviceBuffer {
