@@ -194,6 +194,21 @@ int qlb_plan_destroy(qlb_plan_t plan);
 int qlb_engine_norm_sq(qlb_engine_t e, double* out);
 int qlb_engine_prob_one(qlb_engine_t e, uint32_t qubit, double* out);
 int qlb_engine_expect_z(qlb_engine_t e, double* out, uint32_t num_qubits);
+/* <Z_q> for every qubit of a complex64 device state, allocating nothing.
+ * No counterpart in the reference.  For callers that must not allocate
+ * device memory while they run -- such as a serving loop that admits
+ * requests by accounting all free HBM to resident state vectors, where a
+ * hidden cudaMalloc would escape that accounting and cudaMalloc/cudaFree
+ * would synchronize the device under other requests' kernels.  The
+ * reduction's scratch is a fixed ~176 KiB array inside the library that
+ * every GPU loading the library holds until exit.  Accepts 1..34 qubits
+ * (rejects others with QLB_ERR_INVALID_ARG).  `out` is host memory for
+ * num_qubits doubles; the call runs on `cuda_stream` and waits for it.
+ * All calls share the scratch: calls whose kernels overlap on the GPU race,
+ * so serialize them.  The first call on a device looks up the scratch's
+ * device address with that device current; make it before any stream
+ * capture starts. */
+int qlb_expect_z_noalloc(const void* state_float2, uint32_t num_qubits, double* out, void* cuda_stream);
 /* Draws `shots` basis states from |amp|^2 with a counter-based generator
  * keyed by `seed`; identical seeds give identical samples on any launch. */
 int qlb_engine_sample(qlb_engine_t e, uint64_t seed, uint64_t shots, uint64_t* out);
