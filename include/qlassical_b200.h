@@ -188,6 +188,13 @@ int qlb_engine_compile(qlb_engine_t e, const qlb_gate_instr* program, uint64_t c
 int qlb_engine_run(qlb_engine_t e, qlb_plan_t plan);
 int qlb_plan_stats(qlb_plan_t plan, qlb_exec_stats* out);
 int qlb_plan_destroy(qlb_plan_t plan);
+/* EXPLAIN: runs the planner on the host only (no GPU needed) for a state of
+ * num_qubits and returns the plan as JSON -- steps, passes (tile qubits,
+ * register phases), per-phase ops and their matrices.  Writes at most `cap`
+ * bytes (NUL-terminated) and the full length to *needed. */
+int qlb_describe_plan(uint32_t num_qubits, int mode, int physical_global_swap,
+                      const qlb_gate_instr* program, uint64_t count, const qlb_pool_view* pool,
+                      char* out, uint64_t cap, uint64_t* needed);
 
 /* FP64 reductions over the device state (no reference counterpart except
  * the probability reduction inside apply_measure, :622-630). */

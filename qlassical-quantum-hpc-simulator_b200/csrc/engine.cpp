@@ -192,6 +192,18 @@ uint32_t validate_instr(const qlb_gate_instr& in, uint32_t n, const qlb_pool_vie
     return k;
 }
 
+// Reads (and clears) the flag the tile kernel raises when a bounded wait
+// gives up; the stream must be idle.
+void check_device_error(qlb_engine& e) {
+    if (!e.err_flag.p) return;
+    int flag = 0;
+    check_cuda(cudaMemcpy(&flag, e.err_flag.p, sizeof(int), cudaMemcpyDeviceToHost), "read error flag");
+    if (flag != 0) {
+        check_cuda(cudaMemset(e.err_flag.p, 0, sizeof(int)), "clear error flag");
+        fail(QLB_ERR_TIMEOUT, "a tile pass gave up waiting for its TMA copies; the state is undefined");
+    }
+}
+
 double prob_one(qlb_engine& e, uint32_t mem_qubit) {
     const uint32_t cap = static_cast<uint32_t>(sm_count()) * 4u;
     double* part = static_cast<double*>(e.red_partial.ensure(cap * sizeof(double)));
@@ -468,6 +480,7 @@ static void delete_engine(qlb_engine* e) {
     state_free(e->sv);
     e->red_partial.release();
     e->red_out.release();
+    e->err_flag.release();
     e->staging.release();
     e->host_pinned.release();
     e->host_prog.release();
@@ -596,6 +609,7 @@ int qlb_engine_execute(qlb_engine_t e, const qlb_gate_instr* prog, uint64_t coun
         // the plan's device buffer is freed when `p` goes out of scope; the
         // kernels that read it must have finished by then
         check_cuda(cudaStreamSynchronize(e->stream), "execute sync");
+        check_device_error(*e);
     });
 }
 
@@ -619,6 +633,23 @@ int qlb_engine_run(qlb_engine_t e, qlb_plan_t plan) {
         if (e->sv.dim == 0) fail(QLB_ERR_STATE, "engine has no state vector");
         e->stats = plan->stats;
         run_plan(*e, *plan);
+    });
+}
+
+int qlb_describe_plan(uint32_t n, int mode, int physical, const qlb_gate_instr* prog, uint64_t count,
+                      const qlb_pool_view* pool, char* out, uint64_t cap, uint64_t* needed) {
+    return guarded([&] {
+        if (count && !prog) fail(QLB_ERR_INVALID_ARG, "program is null");
+        if (n > 34) fail(QLB_ERR_INVALID_ARG, "at most 34 qubits");
+        if (mode < QLB_MODE_PLAIN || mode > QLB_MODE_TILED_TC) fail(QLB_ERR_INVALID_ARG, "unknown execution mode");
+        for (uint64_t i = 0; i < count; ++i) validate_instr(prog[i], n, pool);
+        const std::string js = describe_plan_json(PlanConfig{n, mode, physical}, prog, count, pool);
+        if (needed) *needed = js.size() + 1;
+        if (out && cap) {
+            const size_t m = std::min<size_t>(cap - 1, js.size());
+            std::memcpy(out, js.data(), m);
+            out[m] = '\0';
+        }
     });
 }
 
@@ -661,7 +692,11 @@ int qlb_engine_get_mode(qlb_engine_t e, int* mode) {
     return guarded([&] { need(e, "engine"); need(mode, "mode"); *mode = e->mode; });
 }
 int qlb_engine_synchronize(qlb_engine_t e) {
-    return guarded([&] { need(e, "engine"); check_cuda(cudaStreamSynchronize(e->stream), "sync"); });
+    return guarded([&] {
+        need(e, "engine");
+        check_cuda(cudaStreamSynchronize(e->stream), "sync");
+        check_device_error(*e);
+    });
 }
 int qlb_engine_device_state(qlb_engine_t e, void** out) {
     return guarded([&] { need(e, "engine"); need(out, "out"); *out = e->sv.d; });

@@ -63,7 +63,7 @@ struct qlb_engine {
     std::vector<uint8_t> measurements;
     int mode = QLB_MODE_TILED;
     int physical_global_swap = 0;   // execute GLOBAL_SWAP as a data permutation
-    qlb::DeviceBuffer red_partial, red_out, staging;
+    qlb::DeviceBuffer red_partial, red_out, staging, err_flag;   // err_flag: device int set by bounded waits
     qlb::PinnedBuffer host_pinned, host_prog;
     qlb_exec_stats stats{};
     std::vector<double> last_marginals;

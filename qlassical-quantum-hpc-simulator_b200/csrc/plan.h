@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "engine.h"
@@ -19,6 +20,7 @@ enum StepKind : uint8_t {
 
 struct PlanStep {
     uint8_t kind;
+    uint8_t has_tc;     // STEP_PASS: the pass uses tensor-core ops
     uint32_t index;
     qlb_gate_instr instr;
     uint64_t mat_off;   // float2 offset of a dense matrix in the plan's device buffer
@@ -30,12 +32,21 @@ struct qlb_plan {
     uint32_t n = 0;
     int mode = 0;
     std::vector<qlb::PlanStep> steps;
-    qlb::DeviceBuffer dev;   // [passes | phases | ops | phase words | tile mats | plain mats]
-    size_t o_pass = 0, o_phase = 0, o_ops = 0, o_pd = 0, o_mat = 0, o_plain = 0;
+    qlb::DeviceBuffer dev;   // [passes | phases | ops | matrices]
+    size_t o_pass = 0, o_phase = 0, o_ops = 0, o_mat = 0;
     qlb_exec_stats stats{};
 };
 
 namespace qlb {
+// What the planner needs to know about the engine.
+struct PlanConfig {
+    uint32_t n;
+    int mode;
+    int physical_global_swap;
+};
+// Host-only planning: the plan as JSON (steps, passes, phases, ops, matrices).
+std::string describe_plan_json(const PlanConfig& cfg, const qlb_gate_instr* prog, uint64_t count,
+                               const qlb_pool_view* pool);
 // Builds a plan for the engine's qubit count, mode and options.
 qlb_plan* compile_plan(qlb_engine& e, const qlb_gate_instr* prog, uint64_t count, const qlb_pool_view* pool);
 void run_plan(qlb_engine& e, const qlb_plan& p);

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <complex>
 #include <cstring>
 
 #include "engine.h"
@@ -27,9 +28,9 @@ namespace {
 
 constexpr uint64_t kLowMask = (uint64_t{1} << kLaneLow) - 1;  // memory qubits 0..4
 
-struct Term {            // phase-polynomial term on memory qubits
-    int a, b;            // -1 = absent
-    uint32_t angle;      // turns * 2^32
+struct Term {            // diagonal factor exp(i*angle) on amplitudes whose qubits a (and b) are 1
+    int a, b;            // -1 = absent (a < 0: a global phase)
+    double angle;        // radians
 };
 
 struct MI {              // one instruction mapped to memory qubits
@@ -47,11 +48,11 @@ struct MI {              // one instruction mapped to memory qubits
     const qlb_gate_instr* src = nullptr;
 };
 
-uint32_t turns_u32(double rad) {
-    double t = rad / (2.0 * M_PI);
-    t -= std::floor(t);
-    const double s = std::nearbyint(t * 4294967296.0);
-    return static_cast<uint32_t>(static_cast<uint64_t>(s) & 0xFFFFFFFFull);
+double wrap_angle(double rad) {           // to (-pi, pi]
+    double t = std::fmod(rad, 2.0 * M_PI);
+    if (t <= -M_PI) t += 2.0 * M_PI;
+    if (t > M_PI) t -= 2.0 * M_PI;
+    return t;
 }
 
 uint64_t bitm(uint32_t q) { return uint64_t{1} << q; }
@@ -73,14 +74,14 @@ bool diag_terms(const qlb_pool_view* pool, const MI& mi, std::vector<Term>& out)
                 arg[r] = std::atan2(im, re);
             }
         }
-    out.push_back({-1, -1, turns_u32(arg[0])});
+    out.push_back({-1, -1, (arg[0])});
     if (mi.k == 1) {
-        out.push_back({static_cast<int>(mi.q[0]), -1, turns_u32(arg[1] - arg[0])});
+        out.push_back({static_cast<int>(mi.q[0]), -1, (arg[1] - arg[0])});
     } else {
-        out.push_back({static_cast<int>(mi.q[0]), -1, turns_u32(arg[1] - arg[0])});
-        out.push_back({static_cast<int>(mi.q[1]), -1, turns_u32(arg[2] - arg[0])});
+        out.push_back({static_cast<int>(mi.q[0]), -1, (arg[1] - arg[0])});
+        out.push_back({static_cast<int>(mi.q[1]), -1, (arg[2] - arg[0])});
         out.push_back({static_cast<int>(mi.q[0]), static_cast<int>(mi.q[1]),
-                       turns_u32(arg[3] - arg[2] - arg[1] + arg[0])});
+                       (arg[3] - arg[2] - arg[1] + arg[0])});
     }
     return true;
 }
@@ -105,20 +106,20 @@ MI map_instr(const qlb_gate_instr& in, const Layout& lay, const qlb_pool_view* p
     const double th = static_cast<double>(in.payload.param);
     switch (in.type) {
     case QLB_H: case QLB_Y: case QLB_RX: case QLB_RY: case QLB_X: mi.targets = bitm(mi.q[0]); break;
-    case QLB_Z: mi.diag = true; mi.terms.push_back({static_cast<int>(mi.q[0]), -1, 0x80000000u}); break;
-    case QLB_S: mi.diag = true; mi.terms.push_back({static_cast<int>(mi.q[0]), -1, 0x40000000u}); break;
+    case QLB_Z: mi.diag = true; mi.terms.push_back({static_cast<int>(mi.q[0]), -1, M_PI}); break;
+    case QLB_S: mi.diag = true; mi.terms.push_back({static_cast<int>(mi.q[0]), -1, 0.5 * M_PI}); break;
     case QLB_RZ:
         mi.diag = true;
-        mi.terms.push_back({-1, -1, turns_u32(-0.5 * th)});
-        mi.terms.push_back({static_cast<int>(mi.q[0]), -1, turns_u32(th)});
+        mi.terms.push_back({-1, -1, (-0.5 * th)});
+        mi.terms.push_back({static_cast<int>(mi.q[0]), -1, (th)});
         break;
     case QLB_CZ:
         mi.diag = true;
-        mi.terms.push_back({static_cast<int>(mi.q[0]), static_cast<int>(mi.q[1]), 0x80000000u});
+        mi.terms.push_back({static_cast<int>(mi.q[0]), static_cast<int>(mi.q[1]), M_PI});
         break;
     case QLB_CP:
         mi.diag = true;
-        mi.terms.push_back({static_cast<int>(mi.q[0]), static_cast<int>(mi.q[1]), turns_u32(th)});
+        mi.terms.push_back({static_cast<int>(mi.q[0]), static_cast<int>(mi.q[1]), (th)});
         break;
     case QLB_CX: mi.targets = bitm(mi.q[1]); mi.ctrls = bitm(mi.q[0]); break;
     case QLB_CCX: mi.targets = bitm(mi.q[2]); mi.ctrls = bitm(mi.q[0]) | bitm(mi.q[1]); break;
@@ -191,7 +192,7 @@ void fill_reg(std::vector<int>& reg, bool edge) {
 
 class Planner {
 public:
-    Planner(qlb_engine& e, const qlb_pool_view* pool) : e_(e), pool_(pool), n_(e.sv.n) {}
+    Planner(const PlanConfig& cfg, const qlb_pool_view* pool) : e_(cfg), pool_(pool), n_(cfg.n) {}
 
     std::vector<MI> mi;
     TileProgram prog;
@@ -199,7 +200,6 @@ public:
     qlb_exec_stats stats{};
 
     void plan(const qlb_gate_instr* in, uint64_t count) {
-        if (e_.mode == QLB_MODE_TILED_TC) fail(QLB_ERR_INVALID_ARG, "tensor-core tiled mode is not available in this build");
         const bool tiled = e_.mode != QLB_MODE_PLAIN && n_ >= static_cast<uint32_t>(kTileQubits);
         Layout lay;
         lay.reset();
@@ -322,7 +322,7 @@ public:
     }
 
 private:
-    qlb_engine& e_;
+    PlanConfig e_;
     const qlb_pool_view* pool_;
     uint32_t n_;
 
@@ -413,13 +413,18 @@ private:
             for (int r = 0; r < kRegQubits; ++r) ph.reg_pos[r] = static_cast<uint8_t>(pb.reg[r]);
             choose_threads(pb.reg, edge, ph.thr_pos);
             ph.op_begin = static_cast<uint32_t>(prog.ops.size());
-            encode_ops(pb, P, local_of);
+            encode_ops(pb, P, local_of, pi + 1 == phases.size());
             ph.op_end = static_cast<uint32_t>(prog.ops.size());
             prog.phases.push_back(ph);
         }
         P.phase_end = static_cast<uint32_t>(prog.phases.size());
+        P.n_low = 0;
+        while (P.n_low < kTileQubits && P.tile_pos[P.n_low] == P.n_low) ++P.n_low;
+        P.has_tc = pass_has_tc_ ? 1 : 0;
         PlanStep st{};
         st.kind = STEP_PASS;
+        st.has_tc = P.has_tc;
+        pass_has_tc_ = false;
         st.index = static_cast<uint32_t>(prog.passes.size());
         steps.push_back(st);
         prog.passes.push_back(P);
@@ -446,140 +451,317 @@ private:
         return off;
     }
 
-    void encode_ops(const PhaseBuild& pb, const TilePass&, const int* local_of) {
-        std::vector<Term> run;  // consecutive diagonal instructions merged into one TOP_PHASE
-        auto flush = [&]() {
-            if (!run.empty()) encode_phase(pb, local_of, run);
-            run.clear();
-        };
-        for (uint32_t idx : pb.ops) {
-            const MI& m = mi[idx];
-            if (m.diag) {
-                run.insert(run.end(), m.terms.begin(), m.terms.end());
-                continue;
-            }
-            flush();
-            TileOp op{};
-            for (uint32_t b = 0; b < n_; ++b) {
-                if (!(m.ctrls & bitm(b))) continue;
-                const int r = reg_bit(pb, local_of, b);
-                if (r >= 0) op.ctrl_reg |= 1u << r;
-                else op.ctrl_mem |= bitm(b);
-            }
-            switch (m.type) {
-            case QLB_H: case QLB_Y: case QLB_RX: case QLB_RY: {
-                op.kind = TOP_U1;
-                op.r0 = static_cast<uint8_t>(reg_bit(pb, local_of, m.q[0]));
-                Mat2f g = gate_matrix_1q(m.type, m.param);
-                for (int i = 0; i < 4; ++i) op.m[i] = g.m[i];
-                break;
-            }
-            case QLB_X:
-                op.kind = TOP_X;
-                op.r0 = static_cast<uint8_t>(reg_bit(pb, local_of, m.q[0]));
-                break;
-            case QLB_CX:
-                op.kind = TOP_X;
-                op.r0 = static_cast<uint8_t>(reg_bit(pb, local_of, m.q[1]));
-                break;
-            case QLB_CCX:
-                op.kind = TOP_X;
-                op.r0 = static_cast<uint8_t>(reg_bit(pb, local_of, m.q[2]));
-                break;
-            case QLB_SWAP: case QLB_CSWAP: {
-                const uint32_t a = m.type == QLB_SWAP ? m.q[0] : m.q[1];
-                const uint32_t b = m.type == QLB_SWAP ? m.q[1] : m.q[2];
-                int ra = reg_bit(pb, local_of, a), rb = reg_bit(pb, local_of, b);
-                if (ra > rb) std::swap(ra, rb);
-                op.kind = TOP_SWAP;
-                op.r0 = static_cast<uint8_t>(ra);
-                op.r1 = static_cast<uint8_t>(rb);
-                break;
-            }
-            default: {  // UNITARY / FUSED_BLOCK, non-diagonal, k <= 5
-                const qlb_matrix_entry& e = pool_->metadata[m.matrix_idx];
-                const double* d = pool_->data + 2 * uint64_t{e.offset};
-                if (m.k == 1) {
-                    op.kind = TOP_U1;
-                    op.r0 = static_cast<uint8_t>(reg_bit(pb, local_of, m.q[0]));
-                    for (int i = 0; i < 4; ++i)
-                        op.m[i] = make_float2(static_cast<float>(d[2 * i]), static_cast<float>(d[2 * i + 1]));
-                } else if (m.k == 2) {
-                    int r0 = reg_bit(pb, local_of, m.q[0]), r1 = reg_bit(pb, local_of, m.q[1]);
-                    op.kind = TOP_U2;
-                    op.data = static_cast<uint32_t>(prog.mats.size());
-                    // matrix bit 0 <-> q[0]; the kernel wants bit 0 <-> the lower register bit
-                    const bool flip = r0 > r1;
-                    for (int r = 0; r < 4; ++r)
-                        for (int c = 0; c < 4; ++c) {
-                            auto sw = [&](int x) { return flip ? (((x & 1) << 1) | ((x >> 1) & 1)) : x; };
-                            const int src = sw(r) * 4 + sw(c);
-                            prog.mats.push_back(make_float2(static_cast<float>(d[2 * src]),
-                                                            static_cast<float>(d[2 * src + 1])));
-                        }
-                    if (flip) std::swap(r0, r1);
-                    op.r0 = static_cast<uint8_t>(r0);
-                    op.r1 = static_cast<uint8_t>(r1);
-                } else {
-                    op.kind = (e_.mode == QLB_MODE_TILED_TC && m.k == 5) ? TOP_DENSE_TC : TOP_DENSE;
-                    op.k = static_cast<uint8_t>(m.k);
-                    op.data = push_mat_from_pool(m.matrix_idx);
-                    stats.dense_ops += 1;
-                    if (op.kind == TOP_DENSE_TC) stats.tc_ops += 1;
+    // Accumulated global phase of the pass being built (constant terms of
+    // RZ and diagonal UNITARYs); applied once at the end of its last phase.
+    double pass_global_ = 0.0;
+    bool pass_has_tc_ = false;
+
+    // ---- FP64 form of one register-level op --------------------------------
+    using cd = std::complex<double>;
+    struct HostOp {
+        uint8_t kind = 0;
+        int r0 = 0, r1 = 0, k = 0;
+        uint32_t cm = 0;          // register control mask
+        uint64_t cmem = 0;        // memory control mask (thread dependent)
+        cd m[4];                  // 2x2 (row-major) or m[0] = phase
+        std::vector<cd> mat;      // U2: 4x4 (bit 0 <-> r0 < r1); DENSE: 2^k x 2^k on bits 0..k-1
+        double cost = 0.0;        // CUDA-core instructions per amplitude (planning estimate)
+    };
+
+    std::vector<HostOp> host_ops(const PhaseBuild& pb, const int* local_of, const MI& m) {
+        std::vector<HostOp> out;
+        if (m.diag) {
+            for (const Term& t : m.terms) {
+                if (t.a < 0) {
+                    pass_global_ += t.angle;
+                    continue;
                 }
-                break;
+                HostOp h;
+                h.kind = TOP_CPHASE;
+                const int qs[2] = {t.a, t.b};
+                for (int qq : qs) {
+                    if (qq < 0) continue;
+                    const int r = reg_bit(pb, local_of, static_cast<uint32_t>(qq));
+                    if (r >= 0) h.cm |= 1u << r;
+                    else h.cmem |= bitm(static_cast<uint32_t>(qq));
+                }
+                const double ang = wrap_angle(t.angle);
+                if (ang == 0.0) continue;
+                h.m[0] = std::polar(1.0, ang);
+                h.cost = 1.5;
+                out.push_back(std::move(h));
             }
-            }
-            prog.ops.push_back(op);
+            return out;
         }
-        flush();
+        HostOp h;
+        for (uint32_t b = 0; b < n_; ++b) {
+            if (!(m.ctrls & bitm(b))) continue;
+            const int r = reg_bit(pb, local_of, b);
+            if (r >= 0) h.cm |= 1u << r;
+            else h.cmem |= bitm(b);
+        }
+        const double r2 = 1.0 / std::sqrt(2.0), th = 0.5 * static_cast<double>(m.param);
+        const cd I(0.0, 1.0);
+        switch (m.type) {
+        case QLB_H: h.kind = TOP_U1R; h.m[0] = r2; h.m[1] = r2; h.m[2] = r2; h.m[3] = -r2; h.cost = 2.5; break;
+        case QLB_RY:
+            h.kind = TOP_U1R; h.m[0] = std::cos(th); h.m[1] = -std::sin(th); h.m[2] = std::sin(th); h.m[3] = std::cos(th);
+            h.cost = 2.5;
+            break;
+        case QLB_RX:
+            h.kind = TOP_RX; h.m[0] = std::cos(th); h.m[1] = -I * std::sin(th); h.m[2] = -I * std::sin(th);
+            h.m[3] = std::cos(th); h.cost = 2.5;
+            break;
+        case QLB_Y: h.kind = TOP_U1; h.m[0] = 0.0; h.m[1] = -I; h.m[2] = I; h.m[3] = 0.0; h.cost = 4; break;
+        case QLB_X: case QLB_CX: case QLB_CCX:
+            h.kind = TOP_X;
+            h.m[0] = 0.0; h.m[1] = 1.0; h.m[2] = 1.0; h.m[3] = 0.0;
+            h.cost = 0.5;
+            break;
+        case QLB_SWAP: case QLB_CSWAP: h.kind = TOP_SWAP; h.cost = 0.5; break;
+        default: {
+            const qlb_matrix_entry& e = pool_->metadata[m.matrix_idx];
+            const cd* d = reinterpret_cast<const cd*>(pool_->data + 2 * uint64_t{e.offset});
+            if (m.k == 1) {
+                h.r0 = reg_bit(pb, local_of, m.q[0]);
+                bool real = true;
+                for (int i = 0; i < 4; ++i) {
+                    h.m[i] = d[i];
+                    real = real && d[i].imag() == 0.0;
+                }
+                h.kind = real ? TOP_U1R : TOP_U1;
+                h.cost = real ? 2.5 : 4;
+            } else if (m.k == 2) {
+                int r0 = reg_bit(pb, local_of, m.q[0]), r1 = reg_bit(pb, local_of, m.q[1]);
+                const bool flip = r0 > r1;
+                h.kind = TOP_U2;
+                h.mat.resize(16);
+                for (int r = 0; r < 4; ++r)
+                    for (int c = 0; c < 4; ++c) {
+                        auto sw = [&](int x) { return flip ? (((x & 1) << 1) | ((x >> 1) & 1)) : x; };
+                        h.mat[r * 4 + c] = d[sw(r) * 4 + sw(c)];
+                    }
+                if (flip) std::swap(r0, r1);
+                h.r0 = r0;
+                h.r1 = r1;
+                h.cost = 8;
+            } else {
+                h.kind = TOP_DENSE;
+                h.k = static_cast<int>(m.k);
+                h.mat.assign(d, d + e.num_elements);
+                h.cost = 4.0 * static_cast<double>(1 << m.k);
+            }
+            out.push_back(std::move(h));
+            return out;
+        }
+        }
+        // 1- and 2-qubit standard gates: register targets
+        if (m.type == QLB_SWAP || m.type == QLB_CSWAP) {
+            const uint32_t a = m.type == QLB_SWAP ? m.q[0] : m.q[1];
+            const uint32_t b = m.type == QLB_SWAP ? m.q[1] : m.q[2];
+            int ra = reg_bit(pb, local_of, a), rb = reg_bit(pb, local_of, b);
+            if (ra > rb) std::swap(ra, rb);
+            h.r0 = ra;
+            h.r1 = rb;
+        } else {
+            const uint32_t tq = (m.type == QLB_CX) ? m.q[1] : (m.type == QLB_CCX) ? m.q[2] : m.q[0];
+            h.r0 = reg_bit(pb, local_of, tq);
+        }
+        out.push_back(std::move(h));
+        return out;
     }
 
-    void encode_phase(const PhaseBuild& pb, const int* local_of, const std::vector<Term>& terms) {
-        uint32_t hdr[kPhaseHeaderWords] = {};
-        std::vector<uint32_t> thr, lin;
-        auto pair_index = [](int j, int k) {
-            if (j > k) std::swap(j, k);
-            int idx = 0;
-            for (int a = 0; a < kRegQubits; ++a)
-                for (int b = a + 1; b < kRegQubits; ++b) {
-                    if (a == j && b == k) return idx;
-                    ++idx;
-                }
-            return -1;
-        };
-        for (const Term& t : terms) {
-            if (t.a < 0) {
-                hdr[0] += t.angle;
-                continue;
+    // Applies a uniform (cmem == 0) op to one 5-qubit register vector.
+    static void apply_host(const HostOp& h, cd* v) {
+        const uint32_t cm = h.cm;
+        auto ctl = [&](int i) { return (static_cast<uint32_t>(i) & cm) == cm; };
+        switch (h.kind) {
+        case TOP_U1: case TOP_U1R: case TOP_RX: case TOP_X:
+            for (int i = 0; i < 32; ++i) {
+                if (i & (1 << h.r0) || !ctl(i)) continue;
+                const int j = i | (1 << h.r0);
+                const cd a = v[i], b = v[j];
+                v[i] = h.m[0] * a + h.m[1] * b;
+                v[j] = h.m[2] * a + h.m[3] * b;
             }
-            const int ra = reg_bit(pb, local_of, static_cast<uint32_t>(t.a));
-            const int rb = t.b >= 0 ? reg_bit(pb, local_of, static_cast<uint32_t>(t.b)) : -1;
-            if (t.b < 0) {
-                if (ra >= 0) hdr[1 + ra] += t.angle;
-                else { thr.push_back(static_cast<uint32_t>(t.a) | (0xFFu << 8)); thr.push_back(t.angle); }
-            } else if (ra >= 0 && rb >= 0) {
-                hdr[6 + pair_index(ra, rb)] += t.angle;
-            } else if (ra >= 0) {
-                lin.push_back(static_cast<uint32_t>(ra) | (static_cast<uint32_t>(t.b) << 8));
-                lin.push_back(t.angle);
-            } else if (rb >= 0) {
-                lin.push_back(static_cast<uint32_t>(rb) | (static_cast<uint32_t>(t.a) << 8));
-                lin.push_back(t.angle);
-            } else {
-                thr.push_back(static_cast<uint32_t>(t.a) | (static_cast<uint32_t>(t.b) << 8));
-                thr.push_back(t.angle);
+            break;
+        case TOP_SWAP:
+            for (int i = 0; i < 32; ++i) {
+                if (!(i & (1 << h.r0)) || (i & (1 << h.r1)) || !ctl(i)) continue;
+                std::swap(v[i], v[i ^ (1 << h.r0) ^ (1 << h.r1)]);
+            }
+            break;
+        case TOP_U2:
+            for (int i = 0; i < 32; ++i) {
+                if ((i & ((1 << h.r0) | (1 << h.r1))) || !ctl(i)) continue;
+                const int idx[4] = {i, i | (1 << h.r0), i | (1 << h.r1), i | (1 << h.r0) | (1 << h.r1)};
+                cd in[4], o[4];
+                for (int c = 0; c < 4; ++c) in[c] = v[idx[c]];
+                for (int r = 0; r < 4; ++r) {
+                    o[r] = 0.0;
+                    for (int c = 0; c < 4; ++c) o[r] += h.mat[r * 4 + c] * in[c];
+                }
+                for (int r = 0; r < 4; ++r) v[idx[r]] = o[r];
+            }
+            break;
+        case TOP_DENSE: {
+            const int D = 1 << h.k;
+            for (int g = 0; g < 32; g += D) {
+                cd o[32];
+                for (int r = 0; r < D; ++r) {
+                    o[r] = 0.0;
+                    for (int c = 0; c < D; ++c) o[r] += h.mat[r * D + c] * v[g + c];
+                }
+                for (int r = 0; r < D; ++r) v[g + r] = o[r];
+            }
+            break;
+        }
+        case TOP_CPHASE:
+            for (int i = 0; i < 32; ++i)
+                if (ctl(i)) v[i] *= h.m[0];
+            break;
+        default: break;
+        }
+    }
+
+    void emit_cuda_op(const HostOp& h) {
+        TileOp op{};
+        op.kind = h.kind;
+        op.r0 = static_cast<uint8_t>(h.r0);
+        op.r1 = static_cast<uint8_t>(h.r1);
+        op.ctrl_reg = h.cm;
+        op.ctrl_mem = h.cmem;
+        auto f2 = [](cd z) { return make_float2(static_cast<float>(z.real()), static_cast<float>(z.imag())); };
+        switch (h.kind) {
+        case TOP_U1: for (int i = 0; i < 4; ++i) op.m[i] = f2(h.m[i]); break;
+        case TOP_U1R: for (int i = 0; i < 4; ++i) op.m[i] = make_float2(static_cast<float>(h.m[i].real()), 0.f); break;
+        case TOP_RX: op.m[0] = make_float2(static_cast<float>(h.m[0].real()), static_cast<float>(-h.m[1].imag())); break;
+        case TOP_CPHASE: {
+            op.m[0] = f2(h.m[0]);
+            if (std::abs(h.m[0] + cd(1.0, 0.0)) < 1e-15) op.flags = 1;
+            break;
+        }
+        case TOP_U2: case TOP_DENSE: {
+            op.k = static_cast<uint8_t>(h.k);
+            op.data = static_cast<uint32_t>(prog.mats.size());
+            for (const cd& z : h.mat) prog.mats.push_back(f2(z));
+            if (prog.mats.size() & 1) prog.mats.push_back(make_float2(0.f, 0.f));
+            if (h.kind == TOP_DENSE) stats.dense_ops += 1;
+            break;
+        }
+        default: break;
+        }
+        prog.ops.push_back(op);
+    }
+
+    static uint16_t bf16_rn(float f) {
+        uint32_t u;
+        std::memcpy(&u, &f, 4);
+        u += 0x7FFFu + ((u >> 16) & 1u);
+        return static_cast<uint16_t>(u >> 16);
+    }
+    static float bf16_f(uint16_t b) {
+        const uint32_t u = static_cast<uint32_t>(b) << 16;
+        float f;
+        std::memcpy(&f, &u, 4);
+        return f;
+    }
+
+    // B operand image (hi 8 KB + lo 8 KB, K-major canonical layout) of the
+    // real embedding of the 32x32 unitary U (row-major, FP64).
+    void emit_tc_op(const std::vector<cd>& U) {
+        const uint32_t off = static_cast<uint32_t>(prog.mats.size());
+        prog.mats.resize(prog.mats.size() + 2048, make_float2(0.f, 0.f));
+        unsigned char* img = reinterpret_cast<unsigned char*>(prog.mats.data() + off);
+        for (int n = 0; n < 64; ++n)
+            for (int kk = 0; kk < 64; ++kk) {
+                const int r = n & 31, c = kk & 31;
+                const cd u = U[r * 32 + c];
+                double x;
+                if (n < 32) x = kk < 32 ? u.real() : -u.imag();
+                else x = kk < 32 ? u.imag() : u.real();
+                const uint16_t hi = bf16_rn(static_cast<float>(x));
+                const uint16_t lo = bf16_rn(static_cast<float>(x - static_cast<double>(bf16_f(hi))));
+                const size_t at = static_cast<size_t>(n / 8) * 1024 + static_cast<size_t>(kk / 8) * 128 +
+                                  static_cast<size_t>(n % 8) * 16 + static_cast<size_t>(kk % 8) * 2;
+                std::memcpy(img + at, &hi, 2);
+                std::memcpy(img + 8192 + at, &lo, 2);
+            }
+        TileOp op{};
+        op.kind = TOP_DENSE_TC;
+        op.k = 5;
+        op.data = off;
+        prog.ops.push_back(op);
+        stats.dense_ops += 1;
+        stats.tc_ops += 1;
+        pass_has_tc_ = true;
+    }
+
+    // Register-local ops waiting to be fused into one tensor-core op.
+    struct Acc {
+        std::vector<HostOp> ops;
+        uint32_t touched = 0;   // register bits acted on non-diagonally
+        double cost = 0.0;
+    };
+
+    void flush(Acc& acc) {
+        if (acc.ops.empty()) return;
+        if (acc.cost < 10.0) {     // cheaper as individual CUDA-core ops
+            for (const HostOp& h : acc.ops) emit_cuda_op(h);
+        } else {
+            std::vector<cd> U(32 * 32, cd(0.0, 0.0));
+            for (int c = 0; c < 32; ++c) {
+                cd col[32];
+                for (int r = 0; r < 32; ++r) col[r] = (r == c) ? cd(1.0, 0.0) : cd(0.0, 0.0);
+                for (const HostOp& h : acc.ops) apply_host(h, col);
+                for (int r = 0; r < 32; ++r) U[r * 32 + c] = col[r];
+            }
+            emit_tc_op(U);
+        }
+        acc = Acc{};
+    }
+
+    static uint32_t nondiag_bits(const HostOp& h) {
+        switch (h.kind) {
+        case TOP_U1: case TOP_U1R: case TOP_RX: case TOP_X: return 1u << h.r0;
+        case TOP_SWAP: case TOP_U2: return (1u << h.r0) | (1u << h.r1);
+        case TOP_DENSE: return (1u << h.k) - 1u;
+        default: return 0u;
+        }
+    }
+
+    void encode_ops(const PhaseBuild& pb, const TilePass&, const int* local_of, bool last_phase) {
+        const bool tc = e_.mode == QLB_MODE_TILED_TC;
+        Acc acc;
+        for (uint32_t idx : pb.ops) {
+            for (HostOp& h : host_ops(pb, local_of, mi[idx])) {
+                if (!tc) {
+                    emit_cuda_op(h);
+                    continue;
+                }
+                if (h.cmem == 0) {                       // uniform over the tile: fusable
+                    acc.touched |= nondiag_bits(h);
+                    acc.cost += h.cost;
+                    acc.ops.push_back(std::move(h));
+                } else if (h.kind == TOP_CPHASE && (h.cm & acc.touched) == 0) {
+                    emit_cuda_op(h);                     // diagonal on untouched bits: commutes with acc
+                } else {
+                    flush(acc);
+                    emit_cuda_op(h);
+                }
             }
         }
-        hdr[16] = static_cast<uint32_t>(thr.size() / 2);
-        hdr[17] = static_cast<uint32_t>(lin.size() / 2);
-        TileOp op{};
-        op.kind = TOP_PHASE;
-        op.data = static_cast<uint32_t>(prog.pdata.size());
-        prog.pdata.insert(prog.pdata.end(), hdr, hdr + kPhaseHeaderWords);
-        prog.pdata.insert(prog.pdata.end(), thr.begin(), thr.end());
-        prog.pdata.insert(prog.pdata.end(), lin.begin(), lin.end());
-        prog.ops.push_back(op);
+        if (tc) flush(acc);
+        if (last_phase) {
+            const double g = wrap_angle(pass_global_);
+            if (g != 0.0) {
+                HostOp h;
+                h.kind = TOP_CPHASE;
+                h.m[0] = std::polar(1.0, g);
+                emit_cuda_op(h);
+            }
+            pass_global_ = 0.0;
+        }
     }
 };
 
@@ -588,7 +770,7 @@ size_t align256(size_t x) { return (x + 255) & ~size_t{255}; }
 }  // namespace
 
 qlb_plan* compile_plan(qlb_engine& e, const qlb_gate_instr* prog, uint64_t count, const qlb_pool_view* pool) {
-    Planner pl(e, pool);
+    Planner pl(PlanConfig{e.sv.n, e.mode, e.physical_global_swap}, pool);
     pl.plan(prog, count);
     TileProgram& tp = pl.prog;
     auto* p = new qlb_plan();
@@ -602,15 +784,13 @@ qlb_plan* compile_plan(qlb_engine& e, const qlb_gate_instr* prog, uint64_t count
         p->o_pass = 0;
         p->o_phase = align256(p->o_pass + tp.passes.size() * sizeof(TilePass));
         p->o_ops = align256(p->o_phase + tp.phases.size() * sizeof(TilePhase));
-        p->o_pd = align256(p->o_ops + tp.ops.size() * sizeof(TileOp));
-        p->o_mat = align256(p->o_pd + tp.pdata.size() * sizeof(uint32_t));
+        p->o_mat = align256(p->o_ops + tp.ops.size() * sizeof(TileOp));
         const size_t total = align256(p->o_mat + tp.mats.size() * sizeof(float2));
         check_cuda(cudaStreamSynchronize(e.stream), "plan staging sync");
         char* h = static_cast<char*>(e.host_prog.ensure(total));
         std::memcpy(h + p->o_pass, tp.passes.data(), tp.passes.size() * sizeof(TilePass));
         std::memcpy(h + p->o_phase, tp.phases.data(), tp.phases.size() * sizeof(TilePhase));
         std::memcpy(h + p->o_ops, tp.ops.data(), tp.ops.size() * sizeof(TileOp));
-        std::memcpy(h + p->o_pd, tp.pdata.data(), tp.pdata.size() * sizeof(uint32_t));
         std::memcpy(h + p->o_mat, tp.mats.data(), tp.mats.size() * sizeof(float2));
         void* d = p->dev.ensure(total);
         check_cuda(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, e.stream), "H2D plan");
@@ -621,8 +801,134 @@ qlb_plan* compile_plan(qlb_engine& e, const qlb_gate_instr* prog, uint64_t count
     return p;
 }
 
+std::string describe_plan_json(const PlanConfig& cfg, const qlb_gate_instr* prog, uint64_t count,
+                               const qlb_pool_view* pool) {
+    Planner pl(cfg, pool);
+    pl.plan(prog, count);
+    std::string out;
+    out.reserve(1 << 16);
+    auto num = [&](double v) {
+        char b[32];
+        std::snprintf(b, sizeof b, "%.17g", v);
+        out += b;
+    };
+    auto u = [&](uint64_t v) { out += std::to_string(v); };
+    out += "{\"n\":";
+    u(cfg.n);
+    out += ",\"mode\":";
+    u(static_cast<uint64_t>(cfg.mode));
+    out += ",\"steps\":[";
+    for (size_t i = 0; i < pl.steps.size(); ++i) {
+        const PlanStep& st = pl.steps[i];
+        if (i) out += ",";
+        out += "{\"kind\":";
+        u(st.kind);
+        out += ",\"index\":";
+        u(st.index);
+        out += ",\"type\":";
+        u(st.instr.type);
+        out += ",\"arity\":";
+        u(st.instr.flags_arity & 0x0F);
+        out += ",\"qubits\":[";
+        for (int j = 0; j < 6; ++j) {
+            if (j) out += ",";
+            u(j < 4 ? st.instr.qubits[j] : st.instr.qubits_ext[j - 4]);
+        }
+        out += "],\"param\":";
+        num(static_cast<double>(st.instr.payload.param));
+        out += ",\"mat\":";
+        u(st.mat_off);
+        out += "}";
+    }
+    out += "],\"passes\":[";
+    for (size_t i = 0; i < pl.prog.passes.size(); ++i) {
+        const TilePass& P = pl.prog.passes[i];
+        if (i) out += ",";
+        out += "{\"tile_pos\":[";
+        for (int j = 0; j < kTileQubits; ++j) {
+            if (j) out += ",";
+            u(P.tile_pos[j]);
+        }
+        out += "],\"n_low\":";
+        u(P.n_low);
+        out += ",\"has_tc\":";
+        u(P.has_tc);
+        out += ",\"phases\":[";
+        for (uint32_t ph = P.phase_begin; ph < P.phase_end; ++ph) {
+            const TilePhase& T = pl.prog.phases[ph];
+            if (ph != P.phase_begin) out += ",";
+            out += "{\"reg_pos\":[";
+            for (int j = 0; j < kRegQubits; ++j) {
+                if (j) out += ",";
+                u(T.reg_pos[j]);
+            }
+            out += "],\"thr_pos\":[";
+            for (int j = 0; j < kThreadQubits; ++j) {
+                if (j) out += ",";
+                u(T.thr_pos[j]);
+            }
+            out += "],\"ops\":[";
+            for (uint32_t o = T.op_begin; o < T.op_end; ++o) {
+                const TileOp& op = pl.prog.ops[o];
+                if (o != T.op_begin) out += ",";
+                out += "{\"kind\":";
+                u(op.kind);
+                out += ",\"r0\":";
+                u(op.r0);
+                out += ",\"r1\":";
+                u(op.r1);
+                out += ",\"k\":";
+                u(op.k);
+                out += ",\"ctrl_reg\":";
+                u(op.ctrl_reg);
+                out += ",\"ctrl_mem\":";
+                u(op.ctrl_mem);
+                out += ",\"flags\":";
+                u(op.flags);
+                out += ",\"data\":";
+                u(op.data);
+                out += ",\"m\":[";
+                for (int j = 0; j < 4; ++j) {
+                    if (j) out += ",";
+                    num(op.m[j].x);
+                    out += ",";
+                    num(op.m[j].y);
+                }
+                out += "]}";
+            }
+            out += "]}";
+        }
+        out += "]}";
+    }
+    out += "],\"mats\":[";
+    for (size_t i = 0; i < pl.prog.mats.size(); ++i) {
+        if (i) out += ",";
+        num(pl.prog.mats[i].x);
+        out += ",";
+        num(pl.prog.mats[i].y);
+    }
+    out += "],\"stats\":{\"sweeps\":";
+    u(pl.stats.sweeps);
+    out += ",\"tile_passes\":";
+    u(pl.stats.tile_passes);
+    out += ",\"tc_ops\":";
+    u(pl.stats.tc_ops);
+    out += ",\"dense_ops\":";
+    u(pl.stats.dense_ops);
+    out += ",\"ops\":";
+    u(pl.prog.ops.size());
+    out += ",\"phases\":";
+    u(pl.prog.phases.size());
+    out += "}}";
+    return out;
+}
+
 void run_plan(qlb_engine& e, const qlb_plan& p) {
     if (p.n != e.sv.n) fail(QLB_ERR_INVALID_ARG, "plan was compiled for a different number of qubits");
+    if (!e.err_flag.p) {
+        e.err_flag.ensure(256);
+        check_cuda(cudaMemsetAsync(e.err_flag.p, 0, sizeof(int), e.stream), "clear error flag");
+    }
     const char* d = static_cast<const char*>(p.dev.p);
     const float2* mats = reinterpret_cast<const float2*>(d + p.o_mat);
     for (const PlanStep& st : p.steps) {
@@ -630,8 +936,9 @@ void run_plan(qlb_engine& e, const qlb_plan& p) {
         case STEP_PASS:
             check_cuda(launch_tile_pass(e.sv.d, e.sv.n, reinterpret_cast<const TilePass*>(d + p.o_pass),
                                         reinterpret_cast<const TilePhase*>(d + p.o_phase),
-                                        reinterpret_cast<const TileOp*>(d + p.o_ops),
-                                        reinterpret_cast<const uint32_t*>(d + p.o_pd), mats, st.index, e.stream),
+                                        reinterpret_cast<const TileOp*>(d + p.o_ops), mats, st.index,
+                                        static_cast<int>(st.has_tc), static_cast<int*>(e.err_flag.p),
+                                        e.stream),
                        "tile pass");
             break;
         case STEP_PLAIN: apply_plain(e, st.instr, mats + st.mat_off); break;

@@ -1,16 +1,20 @@
-// tile.cu -- the register-resident tile kernel (one launch per pass).
+// tile.cu -- the persistent register-resident tile kernel (one launch per pass).
 //
-// Each CTA (256 threads) owns one tile of 2^13 complex64 amplitudes: the
-// amplitudes whose non-tile index bits equal the CTA's tile number.  A
-// thread holds 32 amplitudes in registers (5 "register qubits"), the
-// thread index covers the other 8 tile qubits.  The pass is a list of
-// phases; each phase applies its instructions purely in registers, and
-// consecutive phases re-split the tile qubits by transposing the tile
-// through 64 KB of XOR-swizzled shared memory.  The first phase reads the
-// tile straight from HBM and the last phase writes it straight back; both
-// use lanes = memory qubits 0..4, so every warp request is 256 contiguous
-// bytes.  HBM traffic: 16 B per amplitude per pass, independent of how many
-// instructions the pass absorbs.
+// One CTA per SM (256 threads, ~140 KB shared memory) walks the pass's tiles.
+// Each tile is 2^13 complex64 amplitudes = 2^(13 - n_low) runs of 2^n_low
+// contiguous amplitudes; warp 0 streams the *next* tile into the idle
+// 64 KB buffer with cp.async.bulk (TMA bulk copies, completion counted on an
+// mbarrier) while the CTA computes the current one, so HBM reads overlap
+// compute.  A thread holds 32 amplitudes in registers; the pass's phases
+// apply their ops as register arithmetic and re-split the tile between
+// phases by transposing it through the XOR-swizzled buffer.  The last phase
+// stores straight to HBM (32 consecutive complex64 per warp request).
+// HBM traffic: 16 B per amplitude per pass, however many gates the pass holds.
+//
+// Every mbarrier wait is bounded; on expiry the CTA raises *err, waits (also
+// bounded) for its own copy in flight and returns.
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 #include "tile.h"
 
@@ -21,86 +25,160 @@ namespace {
 constexpr int NT = kTileThreads;            // 256
 constexpr int NR = 1 << kRegQubits;         // 32
 constexpr int TILE = 1 << kTileQubits;      // 8192
+constexpr uint32_t kWaitLimit = 1u << 26;
+constexpr size_t kSmemBuffers = 2 * TILE * sizeof(float2);
+constexpr size_t kSmemOps = kMaxSmemOps * sizeof(TileOp);
+constexpr size_t kSmemPhases = kMaxSmemPhases * sizeof(TilePhase);
+constexpr size_t kSmemMisc = 64;             // 2 TMA mbarriers, MMA mbarrier, TMEM address
+constexpr size_t kSmemTcB = 16384;           // B operand staging of a tensor-core op
+constexpr size_t kSmemTotal = kSmemBuffers + kSmemOps + kSmemPhases + sizeof(TilePass) + kSmemMisc + kSmemTcB;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Gives up after kWaitLimit polls or 2 s, whichever comes first.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    const uint64_t t0 = global_ns();
+    for (uint32_t i = 0; i < kWaitLimit; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 1023u) == 1023u && global_ns() - t0 > 2000000000ull) break;
+    }
+    return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t fold4(uint32_t i) { return ((i >> 4) ^ (i >> 8) ^ (i >> 12)) & 15u; }
 
+__device__ __forceinline__ uint64_t tile_base(const TilePass& P, uint64_t tile) {
+    uint64_t base = 0;
+    for (uint32_t j = 0; j < P.n_out; ++j, tile >>= 1)
+        if (tile & 1u) base |= uint64_t{1} << P.out_mem[j];
+    return base;
+}
+
+// Warp 0 issues the TMA bulk copies of one tile into `dst`.
+__device__ __forceinline__ void issue_tile_load(float2* dst, const float2* __restrict__ state, const TilePass& P,
+                                                uint64_t tile, uint64_t* bar) {
+    const uint32_t lane = threadIdx.x & 31;
+    if (lane == 0) mbar_arrive_expect_tx(bar, TILE * sizeof(float2));
+    __syncwarp();
+    const uint64_t base = tile_base(P, tile);
+    const uint32_t nl = P.n_low;
+    const uint32_t chunks = 1u << (kTileQubits - nl);
+    const uint32_t bytes = (1u << nl) * static_cast<uint32_t>(sizeof(float2));
+    for (uint32_t c = lane; c < chunks; c += 32) {
+        uint64_t g = base;
+        for (uint32_t j = nl; j < static_cast<uint32_t>(kTileQubits); ++j)
+            if ((c >> (j - nl)) & 1u) g |= uint64_t{1} << P.tile_pos[j];
+        bulk_g2s(dst + (static_cast<size_t>(c) << nl), state + g, bytes, bar);
+    }
+}
+
 struct PhaseMap {
-    uint32_t st;          // swizzled shared-memory slot of the thread's register 0
-    uint32_t s[kRegQubits];  // slot offset (XOR) of register bit j
-    uint64_t gt;          // memory index of the thread's register 0
-    uint64_t ge[kRegQubits]; // memory bit of register bit j
+    uint32_t tp;               // tile-local index bits of the thread
+    uint32_t e[kRegQubits];    // tile-local bit of register bit j
+    uint32_t st;               // swizzled slot of (thread, register 0)
+    uint32_t s[kRegQubits];    // swizzled slot offset of register bit j
+    uint64_t gt;               // memory index of (thread, register 0), including the tile base
 };
 
 __device__ __forceinline__ PhaseMap make_map(const TilePass& P, const TilePhase& ph, uint64_t base) {
     PhaseMap M;
-    uint32_t tpart = 0;
-    uint64_t gmem = base;
+    uint32_t tp = 0;
+    uint64_t g = base;
     const uint32_t t = threadIdx.x;
 #pragma unroll
-    for (int j = 0; j < kThreadQubits; ++j) {
+    for (int j = 0; j < kThreadQubits; ++j)
         if ((t >> j) & 1u) {
-            tpart |= 1u << ph.thr_pos[j];
-            gmem |= uint64_t{1} << P.tile_pos[ph.thr_pos[j]];
+            tp |= 1u << ph.thr_pos[j];
+            g |= uint64_t{1} << P.tile_pos[ph.thr_pos[j]];
         }
-    }
-    M.st = tpart ^ fold4(tpart);
-    M.gt = gmem;
+    M.tp = tp;
+    M.st = tp ^ fold4(tp);
+    M.gt = g;
 #pragma unroll
     for (int j = 0; j < kRegQubits; ++j) {
-        const uint32_t e = 1u << ph.reg_pos[j];
-        M.s[j] = e ^ fold4(e);
-        M.ge[j] = uint64_t{1} << P.tile_pos[ph.reg_pos[j]];
+        M.e[j] = 1u << ph.reg_pos[j];
+        M.s[j] = M.e[j] ^ fold4(M.e[j]);
     }
     return M;
 }
 
-__device__ __forceinline__ uint32_t slot_of(const PhaseMap& M, int m) {
-    uint32_t r = M.st;
-    if (m & 1) r ^= M.s[0];
-    if (m & 2) r ^= M.s[1];
-    if (m & 4) r ^= M.s[2];
-    if (m & 8) r ^= M.s[3];
-    if (m & 16) r ^= M.s[4];
+__device__ __forceinline__ uint32_t local_of(const PhaseMap& M, int m) {
+    uint32_t r = M.tp;
+#pragma unroll
+    for (int j = 0; j < kRegQubits; ++j)
+        if ((m >> j) & 1) r |= M.e[j];
     return r;
 }
-
-__device__ __forceinline__ uint64_t gaddr(const PhaseMap& M, int m) {
-    uint64_t r = M.gt;
-    if (m & 1) r |= M.ge[0];
-    if (m & 2) r |= M.ge[1];
-    if (m & 4) r |= M.ge[2];
-    if (m & 8) r |= M.ge[3];
-    if (m & 16) r |= M.ge[4];
+__device__ __forceinline__ uint32_t slot_of(const PhaseMap& M, int m) {
+    uint32_t r = M.st;
+#pragma unroll
+    for (int j = 0; j < kRegQubits; ++j)
+        if ((m >> j) & 1) r ^= M.s[j];
     return r;
 }
 
 // ---- register operations ------------------------------------------------
 
-template <int R>
-__device__ __forceinline__ void op_u1(float2 (&v)[NR], const float2 (&m)[4], uint32_t cm) {
-#pragma unroll
-    for (int i = 0; i < NR; ++i) {
-        if (i & (1 << R)) continue;
-        const int j = i | (1 << R);
-        if ((static_cast<uint32_t>(i) & cm) == cm) {
-            const float2 a0 = v[i], a1 = v[j];
-            v[i] = cfma(m[1], a1, cmul(m[0], a0));
-            v[j] = cfma(m[3], a1, cmul(m[2], a0));
-        }
-    }
+__device__ __forceinline__ void u1_pair(float2& a0, float2& a1, const float2 (&m)[4]) {
+    const float2 x = a0, y = a1;
+    a0 = cfma(m[1], y, cmul(m[0], x));
+    a1 = cfma(m[3], y, cmul(m[2], x));
+}
+__device__ __forceinline__ void u1r_pair(float2& a0, float2& a1, float m0, float m1, float m2, float m3) {
+    const float2 x = a0, y = a1;
+    a0 = make_float2(fmaf(m1, y.x, m0 * x.x), fmaf(m1, y.y, m0 * x.y));
+    a1 = make_float2(fmaf(m3, y.x, m2 * x.x), fmaf(m3, y.y, m2 * x.y));
+}
+__device__ __forceinline__ void rx_pair(float2& a0, float2& a1, float c, float s) {
+    const float2 x = a0, y = a1;
+    a0 = make_float2(fmaf(s, y.y, c * x.x), fmaf(-s, y.x, c * x.y));
+    a1 = make_float2(fmaf(s, x.y, c * y.x), fmaf(-s, x.x, c * y.y));
 }
 
-template <int R>
-__device__ __forceinline__ void op_x(float2 (&v)[NR], uint32_t cm) {
+// Pair loops over register bit R; the common cm = 0 case has no predicates.
+template <int R, typename F>
+__device__ __forceinline__ void for_pairs(float2 (&v)[NR], uint32_t cm, F&& f) {
+    if (cm == 0) {
 #pragma unroll
-    for (int i = 0; i < NR; ++i) {
-        if (i & (1 << R)) continue;
-        const int j = i | (1 << R);
-        if ((static_cast<uint32_t>(i) & cm) == cm) {
-            const float2 t = v[i];
-            v[i] = v[j];
-            v[j] = t;
-        }
+        for (int i = 0; i < NR; ++i)
+            if (!(i & (1 << R))) f(v[i], v[i | (1 << R)]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < NR; ++i)
+            if (!(i & (1 << R)) && ((static_cast<uint32_t>(i) & cm) == cm)) f(v[i], v[i | (1 << R)]);
     }
 }
 
@@ -128,7 +206,7 @@ __device__ __forceinline__ void op_u2(float2 (&v)[NR], const float2* __restrict_
         if (i & ((1 << R0) | (1 << R1))) continue;
         if ((static_cast<uint32_t>(i) & cm) != cm) continue;
         const int idx[4] = {i, i | (1 << R0), i | (1 << R1), i | (1 << R0) | (1 << R1)};
-        float2 in[4], out[4];
+        float2 in[4];
 #pragma unroll
         for (int c = 0; c < 4; ++c) in[c] = v[idx[c]];
 #pragma unroll
@@ -136,15 +214,11 @@ __device__ __forceinline__ void op_u2(float2 (&v)[NR], const float2* __restrict_
             float2 acc = cmul(M[r * 4], in[0]);
 #pragma unroll
             for (int c = 1; c < 4; ++c) acc = cfma(M[r * 4 + c], in[c], acc);
-            out[r] = acc;
+            v[idx[r]] = acc;
         }
-#pragma unroll
-        for (int r = 0; r < 4; ++r) v[idx[r]] = out[r];
     }
 }
 
-// Dense 2^K x 2^K on register bits 0..K-1 (K = 3, 4): groups of 2^K
-// consecutive registers.
 template <int K>
 __device__ __forceinline__ void op_dense_reg(float2 (&v)[NR], const float2* __restrict__ mat) {
     constexpr int D = 1 << K;
@@ -168,11 +242,11 @@ __device__ __forceinline__ void op_dense_reg(float2 (&v)[NR], const float2* __re
     }
 }
 
-// Dense 32 x 32 on all five register bits; outputs are parked in the
-// thread's own shared-memory slots (no other thread touches them during a
-// phase) to keep register pressure bounded.
+// Dense 32 x 32 on all five register bits; the outputs are parked in the
+// slots this thread owns in the current layout (`linear` in the first phase,
+// swizzled afterwards), which no other thread touches during the phase.
 __device__ __forceinline__ void op_dense5(float2 (&v)[NR], const float2* __restrict__ mat, float2* sm,
-                                          const PhaseMap& M) {
+                                          const PhaseMap& M, bool linear) {
 #pragma unroll 1
     for (int r = 0; r < NR; ++r) {
         const float4* row = reinterpret_cast<const float4*>(mat + r * NR);
@@ -183,80 +257,172 @@ __device__ __forceinline__ void op_dense5(float2 (&v)[NR], const float2* __restr
             acc = cfma(make_float2(w.x, w.y), v[c], acc);
             acc = cfma(make_float2(w.z, w.w), v[c + 1], acc);
         }
-        uint32_t sl = M.st;
+        uint32_t sl = linear ? M.tp : M.st;
 #pragma unroll
         for (int j = 0; j < kRegQubits; ++j)
-            if ((r >> j) & 1) sl ^= M.s[j];
+            if ((r >> j) & 1) sl = linear ? (sl | M.e[j]) : (sl ^ M.s[j]);
         sm[sl] = acc;
     }
 #pragma unroll
-    for (int m = 0; m < NR; ++m) {
-        uint32_t sl = M.st;
-#pragma unroll
-        for (int j = 0; j < kRegQubits; ++j)
-            if ((m >> j) & 1) sl ^= M.s[j];
-        v[m] = sm[sl];
-    }
+    for (int m = 0; m < NR; ++m) v[m] = sm[linear ? local_of(M, m) : slot_of(M, m)];
 }
 
-// Phase polynomial.  Layout of pdata (uint32) at op.data:
-//   [0] constant angle, [1..5] unconditional h_j, [6..15] q_{jk} (j<k,
-//   lexicographic), [16] number of thread terms T, [17] number of linear
-//   conditional terms L, then T words (ga | gb << 8) + T angles, then
-//   L words (j | gb << 8) + L angles.  Angles are turns * 2^32.
-__device__ __forceinline__ void op_phase(float2 (&v)[NR], const uint32_t* __restrict__ pd, uint64_t gt) {
-    uint32_t acc = __ldg(pd + 0);
-    uint32_t h[kRegQubits], q[10];
+// ---- tensor-core dense op (tcgen05) ----------------------------------------
+//
+// A 32x32 complex unitary U on the five register qubits, applied to all 256
+// register groups of the tile at once:  D = A * B^T with
+//   A[row t][k]  = x_t[k],   x_t = (Re a_0..Re a_31, Im a_0..Im a_31)  (thread t = row t)
+//   B[n][k]      = real embedding of U: [[Re U, -Im U], [Im U, Re U]]
+// in bf16 split precision: D = Ahi*Bhi + Ahi*Blo + Alo*Bhi, FP32 accumulate
+// in tensor memory (rows 0..127 -> TMEM columns 0..63, rows 128..255 ->
+// columns 64..127).  Both operands use the K-major, no-swizzle canonical
+// layout: 8 x 16 B core matrices, LBO = 128 B between the K chunks of one
+// row group, SBO = 1024 B between 8-row groups (K = 64 -> 8 chunks).
+constexpr uint32_t kTcCols = 128;
+constexpr uint32_t kTcBBytes = 16384;          // B hi (8 KB) + B lo (8 KB)
+constexpr uint32_t kTcIdesc = (1u << 4)        // D format F32
+                              | (1u << 7)      // A format BF16
+                              | (1u << 10)     // B format BF16
+                              | ((64u >> 3) << 17)    // N = 64
+                              | ((128u >> 4) << 24);  // M = 128
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t smem_addr) {
+    return static_cast<uint64_t>((smem_addr >> 4) & 0x3FFFu) | (static_cast<uint64_t>(128u >> 4) << 16) |
+           (static_cast<uint64_t>(1024u >> 4) << 32) | (uint64_t{1} << 46);
+}
+
+__device__ __forceinline__ uint32_t bf16_bits_rn(float x) {
+    return static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16_rn(x)));
+}
+__device__ __forceinline__ float bf16_to_float(uint32_t b) { return __uint_as_float(b << 16); }
+
+// Writes this thread's row of A (hi and lo) into the canonical layout.
+__device__ __forceinline__ void tc_write_a(const float2 (&v)[NR], unsigned char* a_hi, unsigned char* a_lo) {
+    const uint32_t t = threadIdx.x;
+    const uint32_t rowoff = (t >> 3) * 1024u + (t & 7u) * 16u;
 #pragma unroll
-    for (int j = 0; j < kRegQubits; ++j) h[j] = __ldg(pd + 1 + j);
+    for (int c = 0; c < 8; ++c) {           // K chunk c = reals 8c .. 8c+7
+        uint32_t hi[4], lo[4];
 #pragma unroll
-    for (int j = 0; j < 10; ++j) q[j] = __ldg(pd + 6 + j);
-    const uint32_t T = __ldg(pd + 16), L = __ldg(pd + 17);
-    const uint32_t* tw = pd + 18;
-    for (uint32_t i = 0; i < T; ++i) {
-        const uint32_t w = __ldg(tw + 2 * i), ang = __ldg(tw + 2 * i + 1);
-        const uint32_t ga = w & 0xFFu, gb = (w >> 8) & 0xFFu;
-        const bool on = ((gt >> ga) & 1u) && (gb == 0xFFu || ((gt >> gb) & 1u));
-        acc += on ? ang : 0u;
-    }
-    const uint32_t* lw = tw + 2 * T;
-    for (uint32_t i = 0; i < L; ++i) {
-        const uint32_t w = __ldg(lw + 2 * i), ang = __ldg(lw + 2 * i + 1);
-        const uint32_t j = w & 0xFFu, gb = (w >> 8) & 0xFFu;
-        const uint32_t add = (gb == 0xFFu || ((gt >> gb) & 1u)) ? ang : 0u;
-#pragma unroll
-        for (int jj = 0; jj < kRegQubits; ++jj) h[jj] += (j == static_cast<uint32_t>(jj)) ? add : 0u;
-    }
-    constexpr float kTurnToRad = 6.283185307179586f / 4294967296.0f;
-#pragma unroll
-    for (int m = 0; m < NR; ++m) {
-        uint32_t phi = acc;
-#pragma unroll
-        for (int j = 0; j < kRegQubits; ++j)
-            if ((m >> j) & 1) phi += h[j];
-        int pi = 0;
-#pragma unroll
-        for (int j = 0; j < kRegQubits; ++j)
-#pragma unroll
-            for (int k = j + 1; k < kRegQubits; ++k) {
-                if (((m >> j) & 1) && ((m >> k) & 1)) phi += q[pi];
-                ++pi;
-            }
-        if (phi != 0u) {
-            float sn, cs;
-            __sincosf(static_cast<float>(static_cast<int32_t>(phi)) * kTurnToRad, &sn, &cs);
-            v[m] = cmul(v[m], make_float2(cs, sn));
+        for (int e = 0; e < 4; ++e) {
+            const int k0 = c * 8 + 2 * e;
+            const float x0 = k0 < 32 ? v[k0].x : v[k0 - 32].y;
+            const float x1 = (k0 + 1) < 32 ? v[k0 + 1].x : v[k0 + 1 - 32].y;
+            const uint32_t h0 = bf16_bits_rn(x0), h1 = bf16_bits_rn(x1);
+            const uint32_t l0 = bf16_bits_rn(x0 - bf16_to_float(h0)), l1 = bf16_bits_rn(x1 - bf16_to_float(h1));
+            hi[e] = h0 | (h1 << 16);
+            lo[e] = l0 | (l1 << 16);
         }
+        *reinterpret_cast<uint4*>(a_hi + rowoff + c * 128u) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+        *reinterpret_cast<uint4*>(a_lo + rowoff + c * 128u) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
     }
 }
 
-#define QLB_R1(r, STMT)                      \
-    switch (r) {                             \
-    case 0: { constexpr int R = 0; STMT; } break; \
-    case 1: { constexpr int R = 1; STMT; } break; \
-    case 2: { constexpr int R = 2; STMT; } break; \
-    case 3: { constexpr int R = 3; STMT; } break; \
-    default: { constexpr int R = 4; STMT; } break; \
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(d_tmem), "l"(a), "l"(b), "r"(kTcIdesc), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_ld_row(uint32_t taddr, uint32_t (&r)[64]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, "
+        "%32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, "
+        "%48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+          "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+          "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
+          "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+          "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+struct TcCtx {
+    uint32_t tmem;        // TMEM base address (lane 0, column base)
+    uint64_t* bar;        // MMA-completion mbarrier
+    unsigned char* sb;    // 16 KB B staging area
+    uint32_t uses;        // completed TC ops of this CTA (mbarrier parity)
+};
+
+// Applies one TC op; returns false if the MMA wait gave up (all threads agree).
+__device__ __forceinline__ bool op_dense_tc(float2 (&v)[NR], const float2* __restrict__ bimg, float2* cur,
+                                            TcCtx& tc) {
+    unsigned char* a_hi = reinterpret_cast<unsigned char*>(cur);
+    unsigned char* a_lo = a_hi + 32768;
+    // stage B (16 KB) while no one reads shared memory; everyone has read `cur`
+    __syncthreads();
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(bimg);
+        uint4* dst = reinterpret_cast<uint4*>(tc.sb);
+        for (uint32_t i = threadIdx.x; i < kTcBBytes / 16; i += NT) dst[i] = __ldg(src + i);
+    }
+    tc_write_a(v, a_hi, a_lo);
+    fence_proxy_async();      // generic writes of A and B -> visible to the tensor core
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        tc_fence_after();
+        const uint32_t ahi = smem_u32(a_hi), alo = smem_u32(a_lo), bhi = smem_u32(tc.sb), blo = bhi + 8192u;
+        const uint32_t as[3] = {ahi, ahi, alo}, bs[3] = {bhi, blo, bhi};
+#pragma unroll
+        for (uint32_t mb = 0; mb < 2; ++mb)
+#pragma unroll
+            for (int p = 0; p < 3; ++p)
+#pragma unroll
+                for (uint32_t s = 0; s < 4; ++s)
+                    tc_mma(tc.tmem + mb * 64u, umma_desc(as[p] + mb * 16384u + s * 256u),
+                           umma_desc(bs[p] + s * 256u), (p > 0 || s > 0) ? 1u : 0u);
+        tc_commit(tc.bar);
+    }
+    const bool ok = mbar_wait_bounded(tc.bar, tc.uses & 1u);
+    ++tc.uses;
+    if (__syncthreads_or(!ok)) return false;
+    tc_fence_after();
+    const uint32_t w = threadIdx.x >> 5;
+    uint32_t r[64];
+    tc_ld_row(tc.tmem + (((w & 3u) * 32u) << 16) + (w >> 2) * 64u, r);
+#pragma unroll
+    for (int c = 0; c < NR; ++c) v[c] = make_float2(__uint_as_float(r[c]), __uint_as_float(r[32 + c]));
+    tc_fence_before();
+    return true;
+}
+
+template <int CM>
+__device__ __forceinline__ void op_cphase(float2 (&v)[NR], float2 ph) {
+#pragma unroll
+    for (int i = 0; i < NR; ++i)
+        if ((i & CM) == CM) v[i] = cmul(v[i], ph);
+}
+template <int CM>
+__device__ __forceinline__ void op_negate(float2 (&v)[NR]) {
+#pragma unroll
+    for (int i = 0; i < NR; ++i)
+        if ((i & CM) == CM) v[i] = make_float2(-v[i].x, -v[i].y);
+}
+
+#define QLB_R1(r, STMT)                                 \
+    switch (r) {                                        \
+    case 0: { constexpr int R = 0; STMT; } break;       \
+    case 1: { constexpr int R = 1; STMT; } break;       \
+    case 2: { constexpr int R = 2; STMT; } break;       \
+    case 3: { constexpr int R = 3; STMT; } break;       \
+    default: { constexpr int R = 4; STMT; } break;      \
     }
 
 #define QLB_R2(a, b, STMT)                                              \
@@ -273,88 +439,210 @@ __device__ __forceinline__ void op_phase(float2 (&v)[NR], const uint32_t* __rest
     default: { constexpr int A = 3, B = 4; STMT; } break;               \
     }
 
-__device__ __forceinline__ void run_ops(float2 (&v)[NR], const TilePhase& ph, const TileOp* __restrict__ ops,
-                                        const uint32_t* __restrict__ pdata, const float2* __restrict__ mats,
-                                        float2* sm, const PhaseMap& M) {
+#define QLB_CASE_MASK(M, STMT) case M: { constexpr int CM = M; STMT; } break;
+#define QLB_MASK32(cm, STMT)                                                                       \
+    switch (cm) {                                                                                  \
+    QLB_CASE_MASK(0, STMT) QLB_CASE_MASK(1, STMT) QLB_CASE_MASK(2, STMT) QLB_CASE_MASK(3, STMT)     \
+    QLB_CASE_MASK(4, STMT) QLB_CASE_MASK(5, STMT) QLB_CASE_MASK(6, STMT) QLB_CASE_MASK(7, STMT)     \
+    QLB_CASE_MASK(8, STMT) QLB_CASE_MASK(9, STMT) QLB_CASE_MASK(10, STMT) QLB_CASE_MASK(11, STMT)   \
+    QLB_CASE_MASK(12, STMT) QLB_CASE_MASK(13, STMT) QLB_CASE_MASK(14, STMT) QLB_CASE_MASK(15, STMT) \
+    QLB_CASE_MASK(16, STMT) QLB_CASE_MASK(17, STMT) QLB_CASE_MASK(18, STMT) QLB_CASE_MASK(19, STMT) \
+    QLB_CASE_MASK(20, STMT) QLB_CASE_MASK(21, STMT) QLB_CASE_MASK(22, STMT) QLB_CASE_MASK(23, STMT) \
+    QLB_CASE_MASK(24, STMT) QLB_CASE_MASK(25, STMT) QLB_CASE_MASK(26, STMT) QLB_CASE_MASK(27, STMT) \
+    QLB_CASE_MASK(28, STMT) QLB_CASE_MASK(29, STMT) QLB_CASE_MASK(30, STMT)                         \
+    default: { constexpr int CM = 31; STMT; } break;                                               \
+    }
+
+__device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, const TileOp* ops,
+                                        const float2* __restrict__ mats, float2* sm, const PhaseMap& M,
+                                        bool linear, TcCtx& tc) {
     for (uint32_t oi = ph.op_begin; oi < ph.op_end; ++oi) {
         const TileOp& op = ops[oi];
-        const uint8_t kind = op.kind;
-        if (kind == TOP_PHASE) {
-            op_phase(v, pdata + op.data, M.gt);
+        if (op.kind == TOP_DENSE_TC) {      // CTA-wide; never controlled
+            if (!op_dense_tc(v, mats + op.data, sm, tc)) return false;
             continue;
         }
-        if ((M.gt & op.ctrl_mem) != op.ctrl_mem) continue;   // thread-uniform control
+        if ((M.gt & op.ctrl_mem) != op.ctrl_mem) continue;   // thread-uniform condition
         const uint32_t cm = op.ctrl_reg;
-        switch (kind) {
+        switch (op.kind) {
+        case TOP_CPHASE:
+            if (op.flags & 1u) {
+                QLB_MASK32(cm, op_negate<CM>(v));
+            } else {
+                const float2 p = op.m[0];
+                QLB_MASK32(cm, op_cphase<CM>(v, p));
+            }
+            break;
         case TOP_U1: {
-            float2 m[4] = {op.m[0], op.m[1], op.m[2], op.m[3]};
-            QLB_R1(op.r0, op_u1<R>(v, m, cm));
+            const float2 m[4] = {op.m[0], op.m[1], op.m[2], op.m[3]};
+            QLB_R1(op.r0, for_pairs<R>(v, cm, [&](float2& a, float2& b) { u1_pair(a, b, m); }));
             break;
         }
-        case TOP_X: QLB_R1(op.r0, op_x<R>(v, cm)); break;
+        case TOP_U1R: {
+            const float m0 = op.m[0].x, m1 = op.m[1].x, m2 = op.m[2].x, m3 = op.m[3].x;
+            QLB_R1(op.r0, for_pairs<R>(v, cm, [&](float2& a, float2& b) { u1r_pair(a, b, m0, m1, m2, m3); }));
+            break;
+        }
+        case TOP_RX: {
+            const float c = op.m[0].x, s = op.m[0].y;
+            QLB_R1(op.r0, for_pairs<R>(v, cm, [&](float2& a, float2& b) { rx_pair(a, b, c, s); }));
+            break;
+        }
+        case TOP_X:
+            QLB_R1(op.r0, for_pairs<R>(v, cm, [](float2& a, float2& b) {
+                const float2 t = a;
+                a = b;
+                b = t;
+            }));
+            break;
         case TOP_SWAP: QLB_R2(op.r0, op.r1, (op_swap<A, B>(v, cm))); break;
         case TOP_U2: QLB_R2(op.r0, op.r1, (op_u2<A, B>(v, mats + op.data, cm))); break;
         case TOP_DENSE:
             if (op.k == 3) op_dense_reg<3>(v, mats + op.data);
             else if (op.k == 4) op_dense_reg<4>(v, mats + op.data);
-            else op_dense5(v, mats + op.data, sm, M);
+            else op_dense5(v, mats + op.data, sm, M, linear);
             break;
         default: break;
         }
     }
+    return true;
 }
 
 __global__ void __launch_bounds__(NT, 1)
-k_tile_pass(float2* __restrict__ state, const TilePass* __restrict__ passes, const TilePhase* __restrict__ phases,
-            const TileOp* __restrict__ ops, const uint32_t* __restrict__ pdata, const float2* __restrict__ mats,
-            uint32_t pass_index) {
-    extern __shared__ float2 sm[];
-    const TilePass& P = passes[pass_index];
+k_tile_pass(float2* __restrict__ state, const TilePass* __restrict__ passes, const TilePhase* __restrict__ gphases,
+            const TileOp* __restrict__ gops, const float2* __restrict__ mats, uint32_t pass_index,
+            uint64_t ntiles, int has_tc, int* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    float2* bufs = reinterpret_cast<float2*>(smem_raw);
+    TileOp* sops = reinterpret_cast<TileOp*>(smem_raw + kSmemBuffers);
+    TilePhase* sph = reinterpret_cast<TilePhase*>(smem_raw + kSmemBuffers + kSmemOps);
+    TilePass* spass = reinterpret_cast<TilePass*>(smem_raw + kSmemBuffers + kSmemOps + kSmemPhases);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + kSmemBuffers + kSmemOps + kSmemPhases + sizeof(TilePass));
+    uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(bar + 3);
+    unsigned char* sb = smem_raw + kSmemBuffers + kSmemOps + kSmemPhases + sizeof(TilePass) + kSmemMisc;
 
-    // tile base: deposit the CTA index into the non-tile memory qubits
-    uint64_t base = 0;
+    const TilePass& GP = passes[pass_index];
+    // Stage the pass descriptor, its phases and (if they fit) its ops.
     {
-        uint64_t b = blockIdx.x;
-        for (uint32_t j = 0; j < P.n_out; ++j, b >>= 1)
-            if (b & 1u) base |= uint64_t{1} << P.out_mem[j];
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(&GP);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(spass);
+        for (uint32_t i = threadIdx.x; i < sizeof(TilePass) / 4; i += NT) dst[i] = src[i];
     }
-
-    float2 v[NR];
-    const uint32_t pb = P.phase_begin, pe = P.phase_end;
-    PhaseMap M = make_map(P, phases[pb], base);
-#pragma unroll
-    for (int m = 0; m < NR; ++m) v[m] = state[gaddr(M, m)];
-    run_ops(v, phases[pb], ops, pdata, mats, sm, M);
-
-    for (uint32_t p = pb + 1; p < pe; ++p) {
-        __syncthreads();
-#pragma unroll
-        for (int m = 0; m < NR; ++m) sm[slot_of(M, m)] = v[m];
-        __syncthreads();
-        M = make_map(P, phases[p], base);
-#pragma unroll
-        for (int m = 0; m < NR; ++m) v[m] = sm[slot_of(M, m)];
-        run_ops(v, phases[p], ops, pdata, mats, sm, M);
+    const uint32_t pb = GP.phase_begin, pe = GP.phase_end;
+    const uint32_t nph = pe - pb;
+    const bool ph_in_smem = nph <= kMaxSmemPhases;
+    if (ph_in_smem)
+        for (uint32_t i = threadIdx.x; i < nph * sizeof(TilePhase) / 4; i += NT)
+            reinterpret_cast<uint32_t*>(sph)[i] = reinterpret_cast<const uint32_t*>(gphases + pb)[i];
+    const uint32_t ob = gphases[pb].op_begin, oe = gphases[pe - 1].op_end;
+    const bool ops_in_smem = (oe - ob) <= kMaxSmemOps;
+    if (ops_in_smem)
+        for (uint32_t i = threadIdx.x; i < (oe - ob) * sizeof(TileOp) / 4; i += NT)
+            reinterpret_cast<uint32_t*>(sops)[i] = reinterpret_cast<const uint32_t*>(gops + ob)[i];
+    // phase op ranges index the global op array; rebase the shared copy
+    const TilePhase* phases = ph_in_smem ? sph : gphases + pb;
+    const TileOp* ops = ops_in_smem ? sops - ob : gops;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_init(&bar[2], 1);
+        fence_mbar_init();
     }
+    if (has_tc && threadIdx.x < 32) {     // warp 0 owns the tensor-memory allocation
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_holder)),
+                     "r"(kTcCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const TilePass& P = *spass;
+    TcCtx tc{has_tc ? *tmem_holder : 0u, &bar[2], sb, 0u};
+    bool failed = false;
+
+    uint64_t tile = blockIdx.x;
+    if (tile < ntiles && threadIdx.x < 32) issue_tile_load(bufs, state, P, tile, &bar[0]);
+    uint32_t it = 0;
+    for (; tile < ntiles; tile += gridDim.x, ++it) {
+        const uint32_t b = it & 1u;
+        float2* cur = bufs + static_cast<size_t>(b) * TILE;
+        float2* nxt = bufs + static_cast<size_t>(b ^ 1u) * TILE;
+        const uint64_t next = tile + gridDim.x;
+        if (next < ntiles && threadIdx.x < 32) {
+            fence_proxy_async();   // earlier generic-proxy reads of nxt precede the async-proxy writes
+            issue_tile_load(nxt, state, P, next, &bar[b ^ 1u]);
+        }
+        const bool ok = mbar_wait_bounded(&bar[b], (it >> 1) & 1u);
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicExch(err, 1);
+            if (next < ntiles) mbar_wait_bounded(&bar[b ^ 1u], ((it + 1) >> 1) & 1u);
+            failed = true;
+            break;
+        }
+        const uint64_t base = tile_base(P, tile);
+        float2 v[NR];
+        PhaseMap M = make_map(P, phases[0], base);
 #pragma unroll
-    for (int m = 0; m < NR; ++m) state[gaddr(M, m)] = v[m];
+        for (int m = 0; m < NR; ++m) v[m] = cur[local_of(M, m)];
+        bool good = run_ops(v, phases[0], ops, mats, cur, M, true, tc);
+        for (uint32_t p = 1; p < nph && good; ++p) {
+            __syncthreads();
+#pragma unroll
+            for (int m = 0; m < NR; ++m) cur[slot_of(M, m)] = v[m];
+            __syncthreads();
+            M = make_map(P, phases[p], base);
+#pragma unroll
+            for (int m = 0; m < NR; ++m) v[m] = cur[slot_of(M, m)];
+            good = run_ops(v, phases[p], ops, mats, cur, M, false, tc);
+        }
+        if (!good) {     // a tensor-core wait gave up (every thread agrees)
+            if (threadIdx.x == 0) atomicExch(err, 2);
+            if (next < ntiles) mbar_wait_bounded(&bar[b ^ 1u], ((it + 1) >> 1) & 1u);
+            failed = true;
+            break;
+        }
+        // store: memory index of (thread, m) = gt | memory bits of m's register bits
+        const TilePhase& last = phases[nph - 1];
+        uint64_t ge[kRegQubits];
+#pragma unroll
+        for (int j = 0; j < kRegQubits; ++j) ge[j] = uint64_t{1} << P.tile_pos[last.reg_pos[j]];
+#pragma unroll
+        for (int m = 0; m < NR; ++m) {
+            uint64_t g = M.gt;
+#pragma unroll
+            for (int j = 0; j < kRegQubits; ++j)
+                if ((m >> j) & 1) g |= ge[j];
+            state[g] = v[m];
+        }
+        __syncthreads();   // everyone is done with `cur` before it is refilled
+    }
+    if (failed && has_tc) mbar_wait_bounded(&bar[2], tc.uses & 1u);   // a late MMA, if any
+    tc_fence_before();
+    __syncthreads();
+    if (has_tc && threadIdx.x < 32) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tc.tmem), "r"(kTcCols) : "memory");
+    }
 }
 
 }  // namespace
 
-cudaError_t launch_tile_pass(float2* state, uint32_t n, const TilePass* d_pass, const TilePhase* d_phases,
-                             const TileOp* d_ops, const uint32_t* d_pdata, const float2* d_mats,
-                             uint32_t pass_index, cudaStream_t s) {
+cudaError_t launch_tile_pass(float2* state, uint32_t n, const TilePass* d_passes, const TilePhase* d_phases,
+                             const TileOp* d_ops, const float2* d_mats, uint32_t pass_index, int has_tc,
+                             int* err, cudaStream_t s) {
     static bool configured = false;
     if (!configured) {
         cudaError_t e = cudaFuncSetAttribute(k_tile_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             TILE * static_cast<int>(sizeof(float2)));
+                                             static_cast<int>(kSmemTotal));
         if (e != cudaSuccess) return e;
         configured = true;
     }
     const uint64_t tiles = uint64_t{1} << (n - kTileQubits);
-    k_tile_pass<<<static_cast<unsigned>(tiles), NT, TILE * sizeof(float2), s>>>(
-        state, d_pass, d_phases, d_ops, d_pdata, d_mats, pass_index);
+    uint64_t grid = static_cast<uint64_t>(sm_count());
+    if (grid > tiles) grid = tiles;
+    k_tile_pass<<<static_cast<unsigned>(grid), NT, kSmemTotal, s>>>(state, d_passes, d_phases, d_ops, d_mats,
+                                                                     pass_index, tiles, has_tc, err);
     return cudaGetLastError();
 }
 

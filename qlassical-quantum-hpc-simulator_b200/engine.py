@@ -101,6 +101,32 @@ def set_device(device: int) -> None:
     call("qlb_set_device", int(device))
 
 
+def describe_plan(program, num_qubits: int, mode: str = "tiled", pool: Optional[UnitaryPool] = None,
+                  physical_global_swap: bool = False) -> dict:
+    """EXPLAIN: the engine's plan for `program` (host-only, no GPU needed)."""
+    import json
+    if isinstance(program, IRModule):
+        pool = program.unitaries()
+        program = program.program()
+    prog = np.ascontiguousarray(program, dtype=_lib.GATE_INSTR_DTYPE)
+    pool = pool if pool is not None else UnitaryPool()
+    pv, keep = pool.view()
+    L = lib()
+    fn = L.qlb_describe_plan
+    fn.argtypes = [ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
+                   ctypes.POINTER(_lib.PoolView), ctypes.c_char_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]
+    fn.restype = ctypes.c_int
+    m = MODES[mode] if isinstance(mode, str) else int(mode)
+    need = ctypes.c_uint64()
+    _lib.check(fn(num_qubits, m, int(physical_global_swap), _lib.ptr(prog), prog.size, ctypes.byref(pv), None, 0,
+                  ctypes.byref(need)))
+    buf = ctypes.create_string_buffer(need.value)
+    _lib.check(fn(num_qubits, m, int(physical_global_swap), _lib.ptr(prog), prog.size, ctypes.byref(pv), buf,
+                  need.value, ctypes.byref(need)))
+    del keep
+    return json.loads(buf.value.decode())
+
+
 class CUDAEngine:
     """ExecutionEngine on one B200.
 

@@ -1,0 +1,114 @@
+"""CPU emulation of an engine plan (qlb_describe_plan JSON), for testing the
+planner without a GPU.  Each op is applied to the full complex128 state with
+the same meaning the tile kernel gives it: register bit j of a phase is memory
+qubit tile_pos[reg_pos[j]]; ctrl_mem are memory-qubit controls.  Tensor-core
+ops are decoded from their bf16 hi/lo B-operand image, so the emulation sees
+the same split-precision unitary the tensor cores use."""
+from __future__ import annotations
+
+import numpy as np
+
+TOP_U1, TOP_X, TOP_SWAP, TOP_U2, TOP_DENSE, TOP_U1R, TOP_RX, TOP_CPHASE, TOP_DENSE_TC = range(1, 10)
+STEP_PASS, STEP_PLAIN, STEP_MEASURE, STEP_SWAP = range(4)
+
+
+def apply_k(st, n, qubits, mat, ctrl_mask=0):
+    """Dense 2^k matrix on `qubits` (matrix bit j <-> qubits[j]) where all
+    bits of ctrl_mask are set."""
+    k = len(qubits)
+    idx = np.arange(1 << n, dtype=np.int64)
+    zero = np.ones(idx.shape, dtype=bool)
+    for q in qubits:
+        zero &= ((idx >> q) & 1) == 0
+    zero &= (idx & ctrl_mask) == ctrl_mask
+    base = idx[zero]
+    offs = np.array([sum(((j >> b) & 1) << qubits[b] for b in range(k)) for j in range(1 << k)], dtype=np.int64)
+    g = base[:, None] | offs[None, :]
+    st[g] = st[g] @ np.asarray(mat).T
+
+
+def emulate(plan, init=None):
+    n = plan["n"]
+    st = np.zeros(1 << n, dtype=np.complex128)
+    if init is None:
+        st[0] = 1.0
+    else:
+        st[:] = init
+    m2 = np.array(plan["mats"], dtype=np.float64).reshape(-1, 2) if plan["mats"] else np.zeros((0, 2))
+    mats = m2[:, 0] + 1j * m2[:, 1] if len(m2) else np.zeros(0, dtype=np.complex128)
+    for step in plan["steps"]:
+        kind = step["kind"]
+        if kind == STEP_PASS:
+            P = plan["passes"][step["index"]]
+            tp = P["tile_pos"]
+            for ph in P["phases"]:
+                mq = [tp[r] for r in ph["reg_pos"]]
+                for op in ph["ops"]:
+                    cmask = int(op["ctrl_mem"])
+                    for j in range(5):
+                        if (op["ctrl_reg"] >> j) & 1:
+                            cmask |= 1 << mq[j]
+                    m = np.array(op["m"]).reshape(4, 2)
+                    mc = m[:, 0] + 1j * m[:, 1]
+                    kd = op["kind"]
+                    if kd == TOP_U1:
+                        apply_k(st, n, [mq[op["r0"]]], mc.reshape(2, 2), cmask)
+                    elif kd == TOP_U1R:
+                        apply_k(st, n, [mq[op["r0"]]], m[:, 0].reshape(2, 2), cmask)
+                    elif kd == TOP_RX:
+                        c, s = m[0]
+                        apply_k(st, n, [mq[op["r0"]]], np.array([[c, -1j * s], [-1j * s, c]]), cmask)
+                    elif kd == TOP_X:
+                        apply_k(st, n, [mq[op["r0"]]], np.array([[0, 1], [1, 0]]), cmask)
+                    elif kd == TOP_SWAP:
+                        sw = np.eye(4)[[0, 2, 1, 3]]
+                        apply_k(st, n, [mq[op["r0"]], mq[op["r1"]]], sw, cmask)
+                    elif kd == TOP_U2:
+                        apply_k(st, n, [mq[op["r0"]], mq[op["r1"]]], mats[op["data"]:op["data"] + 16].reshape(4, 4),
+                                cmask)
+                    elif kd == TOP_DENSE:
+                        k = op["k"]
+                        D = 1 << k
+                        apply_k(st, n, mq[:k], mats[op["data"]:op["data"] + D * D].reshape(D, D), cmask)
+                    elif kd == TOP_DENSE_TC:
+                        apply_k(st, n, mq[:5], decode_tc_flat(plan, op["data"]), 0)
+                    elif kd == TOP_CPHASE:
+                        idx = np.arange(1 << n, dtype=np.int64)
+                        sel = (idx & cmask) == cmask
+                        st[sel] *= (-1.0 if op["flags"] & 1 else mc[0])
+                    else:
+                        raise ValueError(f"unknown op kind {kd}")
+        elif kind == STEP_PLAIN:
+            t = step["type"]
+            k = step["arity"]
+            qs = step["qubits"][:max(k, 1)]
+            if t in (0x80, 0xE0):
+                D = 1 << k
+                apply_k(st, n, qs[:k], mats[step["mat"]:step["mat"] + D * D].reshape(D, D))
+            else:
+                raise ValueError(f"plain step of type {t:#x} is not emulated")
+        elif kind == STEP_SWAP:
+            a, b = step["qubits"][:2]
+            apply_k(st, n, [a, b], np.eye(4)[[0, 2, 1, 3]])
+        else:
+            raise ValueError("MEASURE steps are not emulated")
+    return st
+
+
+_tc_cache = {}
+
+
+def decode_tc_flat(plan, data):
+    key = (id(plan), data)
+    if key not in _tc_cache:
+        flat = np.array(plan["mats"], dtype=np.float32)   # float2 slots as float pairs
+        raw = flat[2 * data:2 * data + 4096].tobytes()
+        u16 = np.frombuffer(raw, dtype=np.uint16).astype(np.uint32)
+        nn = np.arange(64)[:, None]
+        kk = np.arange(64)[None, :]
+        at = (nn // 8) * 1024 + (kk // 8) * 128 + (nn % 8) * 16 + (kk % 8) * 2
+        hi = (u16[at // 2] << 16).astype(np.uint32).view(np.float32).astype(np.float64)
+        lo = (u16[(8192 + at) // 2] << 16).astype(np.uint32).view(np.float32).astype(np.float64)
+        B = hi + lo
+        _tc_cache[key] = B[:32, :32] + 1j * B[32:, :32]
+    return _tc_cache[key]

@@ -17,7 +17,7 @@ pytestmark = pytest.mark.gpu
 
 MAX_DIFF = 2e-5
 MAX_INFID = 1e-6
-MODES = ["plain", "tiled"]
+MODES = ["plain", "tiled", "tiled_tc"]
 CASES = load_cases()
 
 
@@ -103,7 +103,38 @@ def test_plain_and_tiled_agree_at_24_qubits():
     m = zoo.random_circuit(24, 400, seed=24, types=zoo.REF_TYPES + zoo.EXT_TYPES, max_dense=5)
     a = run_engine(m, "plain").state()
     b = run_engine(m, "tiled").state()
+    c = run_engine(m, "tiled_tc").state()
     check_close(a, b)
+    check_close(a, c)
+
+
+@pytest.mark.parametrize("qubits", [[5, 6, 7, 8, 9], [9, 2, 12, 7, 0], [13, 1, 4, 10, 6]])
+def test_tensor_core_dense5_vs_oracle(qubits):
+    """One random 5-qubit unitary (a tensor-core op) on a random 14-qubit state."""
+    rng = np.random.default_rng(sum(qubits))
+    qc = QuantumCircuit(14)
+    qc.unitary(qubits, zoo.random_unitary(5, rng))
+    m = qc.release()
+    init = zoo.random_state(14, 3)
+    ref, _ = oracle.run_oracle(m, init=init)
+    e = q.CUDAEngine(initial_state=init, mode="tiled_tc")
+    e.execute(m)
+    assert e.last_stats()["tc_ops"] >= 1
+    check_close(ref, e.state())
+
+
+def test_tensor_core_phase_fusion_vs_oracle():
+    """Many gates on a few qubits: the planner fuses each register phase into
+    tensor-core unitaries; thread-dependent CZs split them."""
+    m = circuits.random_rot_cz(16, 10, seed=4)
+    ref, _ = oracle.run_oracle(m)
+    e = q.CUDAEngine(16, mode="tiled_tc")
+    e.execute(m)
+    assert e.last_stats()["tc_ops"] >= 1
+    check_close(ref, e.state())
+    m2 = zoo.random_circuit(15, 400, seed=77, types=["h", "rx", "ry", "rz", "cz", "cx", "u2", "s", "y"])
+    ref2, _ = oracle.run_oracle(m2)
+    check_close(ref2, run_engine(m2, "tiled_tc").state())
 
 
 def test_measurement_seed_determinism_and_reset():

@@ -1,0 +1,66 @@
+"""The tile planner checked on the CPU: its plan (qlb_describe_plan) is
+replayed op by op in FP64 by tests/plan_emulator.py and compared with the
+oracle.  This covers pass formation, register phases, qubit mapping, control
+masks, phase encoding and tensor-core fusion without a GPU."""
+import numpy as np
+import pytest
+
+from qlassical_b200 import circuits
+from qlassical_b200.engine import describe_plan
+from oracle import oracle
+from plan_emulator import emulate
+import zoo
+
+TOL = {"tiled": 2e-5, "tiled_tc": 5e-5}
+
+
+def check(module, mode, init=None, physical=False):
+    plan = describe_plan(module, module.num_qubits, mode, physical_global_swap=physical)
+    want, _ = oracle.run_oracle(module, init=init)
+    got = emulate(plan, init=init)
+    d = oracle.max_abs_diff(want, got)
+    assert d < TOL[mode], d
+    assert oracle.infidelity(want, got) < 1e-6
+    return plan
+
+
+@pytest.mark.parametrize("mode", ["tiled", "tiled_tc"])
+@pytest.mark.parametrize("n", [13, 14, 16])
+def test_zoo_all_types(n, mode):
+    m = zoo.random_circuit(n, 250, seed=n, types=zoo.REF_TYPES + zoo.EXT_TYPES, max_dense=5)
+    check(m, mode)
+
+
+@pytest.mark.parametrize("mode", ["tiled", "tiled_tc"])
+def test_rotation_cz_circuit_uses_tensor_cores(mode):
+    m = circuits.random_rot_cz(16, 8, seed=2)
+    plan = check(m, mode)
+    if mode == "tiled_tc":
+        assert plan["stats"]["tc_ops"] > 0
+    else:
+        assert plan["stats"]["tc_ops"] == 0
+
+
+@pytest.mark.parametrize("mode", ["tiled", "tiled_tc"])
+@pytest.mark.parametrize("physical", [False, True])
+def test_windowed_stream(mode, physical):
+    if not oracle.reference_available():
+        pytest.skip("oracle/_ref not built")
+    m = zoo.random_circuit(15, 150, seed=5, types=["h", "rx", "cx", "swap", "ccx", "cz", "u2"])
+    prog, data, meta = oracle.transpile_reference(m, fusion=False, hw=True, cost_model=1, k_safe=4)
+    win = zoo.module_from_arrays(15, prog, data, meta)
+    plan = describe_plan(win, 15, mode, physical_global_swap=physical)
+    want, _ = oracle.run_oracle(m)
+    assert oracle.max_abs_diff(want, emulate(plan)) < TOL[mode]
+
+
+def test_qft_plan():
+    x = 0b1011011101
+    plan = describe_plan(circuits.qft(14, basis_state=x), 14, "tiled")
+    assert oracle.max_abs_diff(circuits.qft_expected(14, x), emulate(plan)) < 1e-5
+
+
+def test_plain_mode_plan_is_one_step_per_instruction():
+    m = circuits.random_h_rx_cx(14, 3, seed=1)
+    plan = describe_plan(m, 14, "plain")
+    assert len(plan["steps"]) == m.gate_count() and plan["stats"]["tile_passes"] == 0
