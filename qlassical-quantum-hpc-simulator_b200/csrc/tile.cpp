@@ -624,7 +624,43 @@ private:
         }
     }
 
+    // Consecutive pi-phase terms (CZ, Z, ...) are merged into one TOP_SIGNS op:
+    // each term flips the sign of the registers in `pattern` for threads
+    // whose index has all `ctrl_mem` bits set.  Diagonal terms commute, so
+    // merging a run never reorders non-commuting operations.
+    std::vector<std::pair<uint64_t, uint32_t>> sign_run_;
+
+    static uint32_t reg_pattern(uint32_t cm) {
+        uint32_t p = 0;
+        for (uint32_t m = 0; m < 32; ++m)
+            if ((m & cm) == cm) p |= 1u << m;
+        return p;
+    }
+
+    void flush_signs() {
+        if (sign_run_.empty()) return;
+        TileOp op{};
+        op.kind = TOP_SIGNS;
+        if (prog.mats.size() & 1) prog.mats.push_back(make_float2(0.f, 0.f));
+        op.data = static_cast<uint32_t>(prog.mats.size());
+        op.flags = static_cast<uint32_t>(sign_run_.size());
+        for (const auto& t : sign_run_) {
+            uint32_t w[4] = {static_cast<uint32_t>(t.first), static_cast<uint32_t>(t.first >> 32), t.second, 0u};
+            float2 f[2];
+            std::memcpy(f, w, 16);
+            prog.mats.push_back(f[0]);
+            prog.mats.push_back(f[1]);
+        }
+        sign_run_.clear();
+        prog.ops.push_back(op);
+    }
+
     void emit_cuda_op(const HostOp& h) {
+        if (h.kind == TOP_CPHASE && std::abs(h.m[0] + cd(1.0, 0.0)) < 1e-15) {
+            sign_run_.emplace_back(h.cmem, reg_pattern(h.cm));
+            return;
+        }
+        flush_signs();
         TileOp op{};
         op.kind = h.kind;
         op.r0 = static_cast<uint8_t>(h.r0);
@@ -670,6 +706,8 @@ private:
     // B operand image (hi 8 KB + lo 8 KB, K-major canonical layout) of the
     // real embedding of the 32x32 unitary U (row-major, FP64).
     void emit_tc_op(const std::vector<cd>& U) {
+        flush_signs();
+        if (prog.mats.size() & 1) prog.mats.push_back(make_float2(0.f, 0.f));
         const uint32_t off = static_cast<uint32_t>(prog.mats.size());
         prog.mats.resize(prog.mats.size() + 2048, make_float2(0.f, 0.f));
         unsigned char* img = reinterpret_cast<unsigned char*>(prog.mats.data() + off);
@@ -762,6 +800,7 @@ private:
             }
             pass_global_ = 0.0;
         }
+        flush_signs();
     }
 };
 
@@ -900,12 +939,16 @@ std::string describe_plan_json(const PlanConfig& cfg, const qlb_gate_instr* prog
         }
         out += "]}";
     }
+    // the matrix buffer holds float2 matrices and raw words (TC images, sign
+    // terms): dump every 32-bit word as an unsigned integer
     out += "],\"mats\":[";
     for (size_t i = 0; i < pl.prog.mats.size(); ++i) {
+        uint32_t w[2];
+        std::memcpy(w, &pl.prog.mats[i], 8);
         if (i) out += ",";
-        num(pl.prog.mats[i].x);
+        u(w[0]);
         out += ",";
-        num(pl.prog.mats[i].y);
+        u(w[1]);
     }
     out += "],\"stats\":{\"sweeps\":";
     u(pl.stats.sweeps);

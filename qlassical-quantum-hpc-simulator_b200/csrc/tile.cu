@@ -26,7 +26,7 @@ constexpr int NT = kTileThreads;            // 256
 constexpr int NR = 1 << kRegQubits;         // 32
 constexpr int TILE = 1 << kTileQubits;      // 8192
 constexpr uint32_t kWaitLimit = 1u << 26;
-constexpr size_t kSmemBuffers = 2 * TILE * sizeof(float2);
+constexpr size_t kSmemBuffers = 3 * TILE * sizeof(float2);   // 2 TMA buffers + 1 transpose buffer
 constexpr size_t kSmemOps = kMaxSmemOps * sizeof(TileOp);
 constexpr size_t kSmemPhases = kMaxSmemPhases * sizeof(TilePhase);
 constexpr size_t kSmemMisc = 64;             // 2 TMA mbarriers, MMA mbarrier, TMEM address
@@ -87,17 +87,19 @@ __device__ __forceinline__ uint64_t tile_base(const TilePass& P, uint64_t tile) 
     return base;
 }
 
-// Warp 0 issues the TMA bulk copies of one tile into `dst`.
+// All threads issue the TMA bulk copies of one tile into `dst` (one run of
+// 2^n_low amplitudes each); thread 0 registers the expected byte count.  The
+// mbarrier's transaction count may dip below zero when a copy completes
+// before the expectation is registered; the phase still completes only
+// after thread 0's arrival.
 __device__ __forceinline__ void issue_tile_load(float2* dst, const float2* __restrict__ state, const TilePass& P,
                                                 uint64_t tile, uint64_t* bar) {
-    const uint32_t lane = threadIdx.x & 31;
-    if (lane == 0) mbar_arrive_expect_tx(bar, TILE * sizeof(float2));
-    __syncwarp();
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, TILE * sizeof(float2));
     const uint64_t base = tile_base(P, tile);
     const uint32_t nl = P.n_low;
     const uint32_t chunks = 1u << (kTileQubits - nl);
     const uint32_t bytes = (1u << nl) * static_cast<uint32_t>(sizeof(float2));
-    for (uint32_t c = lane; c < chunks; c += 32) {
+    for (uint32_t c = threadIdx.x; c < chunks; c += NT) {
         uint64_t g = base;
         for (uint32_t j = nl; j < static_cast<uint32_t>(kTileQubits); ++j)
             if ((c >> (j - nl)) & 1u) g |= uint64_t{1} << P.tile_pos[j];
@@ -465,6 +467,23 @@ __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, co
         if ((M.gt & op.ctrl_mem) != op.ctrl_mem) continue;   // thread-uniform condition
         const uint32_t cm = op.ctrl_reg;
         switch (op.kind) {
+        case TOP_SIGNS: {
+            // per-thread negate mask over the 32 registers, then sign-bit XORs
+            const uint4* terms = reinterpret_cast<const uint4*>(mats + op.data);
+            uint32_t mask = 0;
+            for (uint32_t t = 0; t < op.flags; ++t) {
+                const uint4 w = __ldg(terms + t);
+                const uint64_t cmem = (static_cast<uint64_t>(w.y) << 32) | w.x;
+                mask ^= ((M.gt & cmem) == cmem) ? w.z : 0u;
+            }
+#pragma unroll
+            for (int m = 0; m < NR; ++m) {
+                const uint32_t sgn = (mask << (31 - m)) & 0x80000000u;
+                v[m].x = __uint_as_float(__float_as_uint(v[m].x) ^ sgn);
+                v[m].y = __uint_as_float(__float_as_uint(v[m].y) ^ sgn);
+            }
+            break;
+        }
         case TOP_CPHASE:
             if (op.flags & 1u) {
                 QLB_MASK32(cm, op_negate<CM>(v));
@@ -562,14 +581,15 @@ k_tile_pass(float2* __restrict__ state, const TilePass* __restrict__ passes, con
     bool failed = false;
 
     uint64_t tile = blockIdx.x;
-    if (tile < ntiles && threadIdx.x < 32) issue_tile_load(bufs, state, P, tile, &bar[0]);
+    float2* xbuf = bufs + 2 * static_cast<size_t>(TILE);
+    if (tile < ntiles) issue_tile_load(bufs, state, P, tile, &bar[0]);
     uint32_t it = 0;
     for (; tile < ntiles; tile += gridDim.x, ++it) {
         const uint32_t b = it & 1u;
         float2* cur = bufs + static_cast<size_t>(b) * TILE;
         float2* nxt = bufs + static_cast<size_t>(b ^ 1u) * TILE;
         const uint64_t next = tile + gridDim.x;
-        if (next < ntiles && threadIdx.x < 32) {
+        if (next < ntiles) {
             fence_proxy_async();   // earlier generic-proxy reads of nxt precede the async-proxy writes
             issue_tile_load(nxt, state, P, next, &bar[b ^ 1u]);
         }
@@ -586,15 +606,20 @@ k_tile_pass(float2* __restrict__ state, const TilePass* __restrict__ passes, con
 #pragma unroll
         for (int m = 0; m < NR; ++m) v[m] = cur[local_of(M, m)];
         bool good = run_ops(v, phases[0], ops, mats, cur, M, true, tc);
+        // Transposes alternate between the transpose buffer and `cur`: the
+        // buffer written at transition k was last read at transition k-2,
+        // before barrier k-1, so one barrier per transition suffices.
+        float2* rbuf = cur;
         for (uint32_t p = 1; p < nph && good; ++p) {
-            __syncthreads();
+            float2* wbuf = (rbuf == xbuf) ? cur : xbuf;
 #pragma unroll
-            for (int m = 0; m < NR; ++m) cur[slot_of(M, m)] = v[m];
+            for (int m = 0; m < NR; ++m) wbuf[slot_of(M, m)] = v[m];
             __syncthreads();
             M = make_map(P, phases[p], base);
 #pragma unroll
-            for (int m = 0; m < NR; ++m) v[m] = cur[slot_of(M, m)];
-            good = run_ops(v, phases[p], ops, mats, cur, M, false, tc);
+            for (int m = 0; m < NR; ++m) v[m] = wbuf[slot_of(M, m)];
+            rbuf = wbuf;
+            good = run_ops(v, phases[p], ops, mats, rbuf, M, false, tc);
         }
         if (!good) {     // a tensor-core wait gave up (every thread agrees)
             if (threadIdx.x == 0) atomicExch(err, 2);

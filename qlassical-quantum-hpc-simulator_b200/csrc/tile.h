@@ -47,7 +47,8 @@ enum TileOpKind : uint8_t {
     TOP_U1R = 6,      // real 2x2 (m[i].x) on register bit r0 (H, RY)
     TOP_RX = 7,       // [[c, -is], [-is, c]] on r0, c = m[0].x, s = m[0].y
     TOP_CPHASE = 8,   // amplitudes with ctrl_reg/ctrl_mem bits all set *= m[0]; flags&1: m[0] == -1
-    TOP_DENSE_TC = 9  // k = 5 on register bits 0..4 on the tensor cores
+    TOP_DENSE_TC = 9, // k = 5 on register bits 0..4 on the tensor cores
+    TOP_SIGNS = 10    // a run of pi phases: flags terms {u64 ctrl_mem, u32 register pattern} at data
 };
 
 struct TileOp {

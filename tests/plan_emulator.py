@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import numpy as np
 
-TOP_U1, TOP_X, TOP_SWAP, TOP_U2, TOP_DENSE, TOP_U1R, TOP_RX, TOP_CPHASE, TOP_DENSE_TC = range(1, 10)
+TOP_U1, TOP_X, TOP_SWAP, TOP_U2, TOP_DENSE, TOP_U1R, TOP_RX, TOP_CPHASE, TOP_DENSE_TC, TOP_SIGNS = range(1, 11)
 STEP_PASS, STEP_PLAIN, STEP_MEASURE, STEP_SWAP = range(4)
 
 
@@ -34,7 +34,8 @@ def emulate(plan, init=None):
         st[0] = 1.0
     else:
         st[:] = init
-    m2 = np.array(plan["mats"], dtype=np.float64).reshape(-1, 2) if plan["mats"] else np.zeros((0, 2))
+    words = np.array(plan["mats"], dtype=np.uint32)             # raw 32-bit words, 2 per float2 slot
+    m2 = words.view(np.float32).astype(np.float64).reshape(-1, 2) if words.size else np.zeros((0, 2))
     mats = m2[:, 0] + 1j * m2[:, 1] if len(m2) else np.zeros(0, dtype=np.complex128)
     for step in plan["steps"]:
         kind = step["kind"]
@@ -72,6 +73,19 @@ def emulate(plan, init=None):
                         apply_k(st, n, mq[:k], mats[op["data"]:op["data"] + D * D].reshape(D, D), cmask)
                     elif kd == TOP_DENSE_TC:
                         apply_k(st, n, mq[:5], decode_tc_flat(plan, op["data"]), 0)
+                    elif kd == TOP_SIGNS:
+                        w = words[2 * op["data"]:2 * op["data"] + 4 * op["flags"]].reshape(-1, 4)
+                        idx = np.arange(1 << n, dtype=np.int64)
+                        reg = np.zeros(idx.shape, dtype=np.int64)
+                        for j in range(5):
+                            reg |= ((idx >> mq[j]) & 1) << j
+                        flip = np.zeros(idx.shape, dtype=bool)
+                        for t in w:
+                            cmem = int(t[0]) | (int(t[1]) << 32)
+                            pat = int(t[2])
+                            hit = ((idx & cmem) == cmem) & (((pat >> reg) & 1) == 1)
+                            flip ^= hit
+                        st[flip] *= -1.0
                     elif kd == TOP_CPHASE:
                         idx = np.arange(1 << n, dtype=np.int64)
                         sel = (idx & cmask) == cmask
@@ -101,7 +115,7 @@ _tc_cache = {}
 def decode_tc_flat(plan, data):
     key = (id(plan), data)
     if key not in _tc_cache:
-        flat = np.array(plan["mats"], dtype=np.float32)   # float2 slots as float pairs
+        flat = np.array(plan["mats"], dtype=np.uint32)    # raw words, 2 per float2 slot
         raw = flat[2 * data:2 * data + 4096].tobytes()
         u16 = np.frombuffer(raw, dtype=np.uint16).astype(np.uint32)
         nn = np.arange(64)[:, None]
