@@ -466,33 +466,11 @@ private:
         cd m[4];                  // 2x2 (row-major) or m[0] = phase
         std::vector<cd> mat;      // U2: 4x4 (bit 0 <-> r0 < r1); DENSE: 2^k x 2^k on bits 0..k-1
         double cost = 0.0;        // CUDA-core instructions per amplitude (planning estimate)
+        bool diag = false;        // diagonal (a phase op), whatever its kind
     };
 
     std::vector<HostOp> host_ops(const PhaseBuild& pb, const int* local_of, const MI& m) {
         std::vector<HostOp> out;
-        if (m.diag) {
-            for (const Term& t : m.terms) {
-                if (t.a < 0) {
-                    pass_global_ += t.angle;
-                    continue;
-                }
-                HostOp h;
-                h.kind = TOP_CPHASE;
-                const int qs[2] = {t.a, t.b};
-                for (int qq : qs) {
-                    if (qq < 0) continue;
-                    const int r = reg_bit(pb, local_of, static_cast<uint32_t>(qq));
-                    if (r >= 0) h.cm |= 1u << r;
-                    else h.cmem |= bitm(static_cast<uint32_t>(qq));
-                }
-                const double ang = wrap_angle(t.angle);
-                if (ang == 0.0) continue;
-                h.m[0] = std::polar(1.0, ang);
-                h.cost = 1.5;
-                out.push_back(std::move(h));
-            }
-            return out;
-        }
         HostOp h;
         for (uint32_t b = 0; b < n_; ++b) {
             if (!(m.ctrls & bitm(b))) continue;
@@ -624,61 +602,49 @@ private:
         }
     }
 
-    // Consecutive pi-phase terms (CZ, Z, ...) are merged into one TOP_SIGNS op:
-    // each term flips the sign of the registers in `pattern` for threads
-    // whose index has all `ctrl_mem` bits set.  Diagonal terms commute, so
-    // merging a run never reorders non-commuting operations.
-    std::vector<std::pair<uint64_t, uint32_t>> sign_run_;
-
-    static uint32_t reg_pattern(uint32_t cm) {
-        uint32_t p = 0;
-        for (uint32_t m = 0; m < 32; ++m)
-            if ((m & cm) == cm) p |= 1u << m;
-        return p;
-    }
-
-    void flush_signs() {
-        if (sign_run_.empty()) return;
-        TileOp op{};
-        op.kind = TOP_SIGNS;
-        if (prog.mats.size() & 1) prog.mats.push_back(make_float2(0.f, 0.f));
-        op.data = static_cast<uint32_t>(prog.mats.size());
-        op.flags = static_cast<uint32_t>(sign_run_.size());
-        for (const auto& t : sign_run_) {
-            uint32_t w[4] = {static_cast<uint32_t>(t.first), static_cast<uint32_t>(t.first >> 32), t.second, 0u};
-            float2 f[2];
-            std::memcpy(f, w, 16);
-            prog.mats.push_back(f[0]);
-            prog.mats.push_back(f[1]);
-        }
-        sign_run_.clear();
-        prog.ops.push_back(op);
-    }
-
     void emit_cuda_op(const HostOp& h) {
-        if (h.kind == TOP_CPHASE && std::abs(h.m[0] + cd(1.0, 0.0)) < 1e-15) {
-            sign_run_.emplace_back(h.cmem, reg_pattern(h.cm));
-            return;
-        }
-        flush_signs();
         TileOp op{};
         op.kind = h.kind;
         op.r0 = static_cast<uint8_t>(h.r0);
         op.r1 = static_cast<uint8_t>(h.r1);
         op.ctrl_reg = h.cm;
         op.ctrl_mem = h.cmem;
+        op.has_mem = h.cmem != 0 ? 1 : 0;
         auto f2 = [](cd z) { return make_float2(static_cast<float>(z.real()), static_cast<float>(z.imag())); };
+        const uint32_t r0 = static_cast<uint32_t>(h.r0);
         switch (h.kind) {
-        case TOP_U1: for (int i = 0; i < 4; ++i) op.m[i] = f2(h.m[i]); break;
-        case TOP_U1R: for (int i = 0; i < 4; ++i) op.m[i] = make_float2(static_cast<float>(h.m[i].real()), 0.f); break;
-        case TOP_RX: op.m[0] = make_float2(static_cast<float>(h.m[0].real()), static_cast<float>(-h.m[1].imag())); break;
-        case TOP_CPHASE: {
-            op.m[0] = f2(h.m[0]);
-            if (std::abs(h.m[0] + cd(1.0, 0.0)) < 1e-15) op.flags = 1;
+        case TOP_U1: case TOP_U1R: case TOP_RX:
+            if (h.cm != 0) {                 // controlled: one complex handler for every 1-qubit kind
+                op.kind = TOP_U1;
+                op.code = static_cast<uint16_t>(OPC_U1_CTL + r0);
+                for (int i = 0; i < 4; ++i) op.m[i] = f2(h.m[i]);
+            } else if (h.kind == TOP_U1) {
+                op.code = static_cast<uint16_t>(OPC_U1 + r0);
+                for (int i = 0; i < 4; ++i) op.m[i] = f2(h.m[i]);
+            } else if (h.kind == TOP_U1R) {
+                op.code = static_cast<uint16_t>(OPC_U1R + r0);
+                for (int i = 0; i < 4; ++i) op.m[i] = make_float2(static_cast<float>(h.m[i].real()), 0.f);
+            } else {
+                op.code = static_cast<uint16_t>(OPC_RX + r0);
+                op.m[0] = make_float2(static_cast<float>(h.m[0].real()), static_cast<float>(-h.m[1].imag()));
+            }
             break;
-        }
+        case TOP_X:
+            op.code = static_cast<uint16_t>((h.cm != 0 ? OPC_X_CTL : OPC_X) + r0);
+            break;
+        case TOP_SWAP:
+            op.code = static_cast<uint16_t>(OPC_SWAP + reg_pair_index(r0, static_cast<uint32_t>(h.r1)));
+            break;
+        case TOP_CPHASE:
+            op.code = OPC_CPHASE;
+            op.m[0] = f2(h.m[0]);
+            break;
         case TOP_U2: case TOP_DENSE: {
             op.k = static_cast<uint8_t>(h.k);
+            op.code = h.kind == TOP_U2 ? static_cast<uint16_t>(OPC_U2 + reg_pair_index(r0, static_cast<uint32_t>(h.r1)))
+                      : h.k == 3       ? static_cast<uint16_t>(OPC_DENSE3)
+                      : h.k == 4       ? static_cast<uint16_t>(OPC_DENSE4)
+                                       : static_cast<uint16_t>(OPC_DENSE5);
             op.data = static_cast<uint32_t>(prog.mats.size());
             for (const cd& z : h.mat) prog.mats.push_back(f2(z));
             if (prog.mats.size() & 1) prog.mats.push_back(make_float2(0.f, 0.f));
@@ -706,7 +672,6 @@ private:
     // B operand image (hi 8 KB + lo 8 KB, K-major canonical layout) of the
     // real embedding of the 32x32 unitary U (row-major, FP64).
     void emit_tc_op(const std::vector<cd>& U) {
-        flush_signs();
         if (prog.mats.size() & 1) prog.mats.push_back(make_float2(0.f, 0.f));
         const uint32_t off = static_cast<uint32_t>(prog.mats.size());
         prog.mats.resize(prog.mats.size() + 2048, make_float2(0.f, 0.f));
@@ -727,6 +692,7 @@ private:
             }
         TileOp op{};
         op.kind = TOP_DENSE_TC;
+        op.code = OPC_DENSE_TC;
         op.k = 5;
         op.data = off;
         prog.ops.push_back(op);
@@ -760,6 +726,7 @@ private:
     }
 
     static uint32_t nondiag_bits(const HostOp& h) {
+        if (h.diag) return 0u;
         switch (h.kind) {
         case TOP_U1: case TOP_U1R: case TOP_RX: case TOP_X: return 1u << h.r0;
         case TOP_SWAP: case TOP_U2: return (1u << h.r0) | (1u << h.r1);
@@ -768,11 +735,225 @@ private:
         }
     }
 
+    // ---- deferred diagonal terms --------------------------------------------
+    // Diagonal gates commute with each other and with every gate whose
+    // targets they do not touch.  Within a pass their phase terms are kept
+    // (keyed by memory-qubit mask) and applied as one TOP_DIAG op only when
+    // a later gate targets one of their qubits, or at the end of the pass.
+    // A term multiplies amplitudes whose mask bits are all set by p1 and the
+    // others by p0 (p0 != 1 only for single-qubit terms such as RZ).
+    struct PTerm {
+        uint64_t mask;
+        cd p1, p0;
+    };
+    std::vector<PTerm> pend_;
+    uint64_t pend_qubits_ = 0;
+
+    void add_pending(uint64_t mask, cd p1, cd p0) {
+        for (PTerm& t : pend_)
+            if (t.mask == mask) {
+                t.p1 *= p1;
+                t.p0 *= p0;
+                return;
+            }
+        pend_.push_back({mask, p1, p0});
+        pend_qubits_ |= mask;
+    }
+
+    void split_mask(const PhaseBuild& pb, const int* local_of, uint64_t mask, uint32_t& cm, uint64_t& cmem) const {
+        cm = 0;
+        cmem = 0;
+        for (uint64_t w = mask; w; w &= w - 1) {
+            const uint32_t q = static_cast<uint32_t>(__builtin_ctzll(w));
+            const int r = reg_bit(pb, local_of, q);
+            if (r >= 0) cm |= 1u << r;
+            else cmem |= bitm(q);
+        }
+    }
+
+    // A register-only term as a (diagonal) accumulator op.
+    static HostOp diag_host_op(uint32_t cm, cd p1, cd p0) {
+        HostOp h;
+        h.diag = true;
+        if (std::abs(p0 - cd(1.0, 0.0)) < 1e-15) {
+            h.kind = TOP_CPHASE;
+            h.cm = cm;
+            h.m[0] = p1;
+            h.cost = 1.5;
+        } else {                                   // single register bit, two phases
+            h.kind = TOP_U1;
+            h.r0 = __builtin_ctz(cm);
+            h.m[0] = p0;
+            h.m[1] = 0.0;
+            h.m[2] = 0.0;
+            h.m[3] = p1;
+            h.cost = 4;
+        }
+        return h;
+    }
+
+    static bool is_one(cd z) { return std::abs(z - cd(1.0, 0.0)) < 1e-15; }
+
+    // Emits the pending terms (and, when `global`, the pass's global phase)
+    // as one TOP_DIAG op in phase `pb`.  With an accumulator (tensor-core
+    // mode) register-only terms join it instead; every pending term commutes
+    // with the accumulator's contents.
+    void flush_pending(const PhaseBuild& pb, const int* local_of, Acc* acc, bool global) {
+        cd R[32];
+        for (cd& z : R) z = cd(1.0, 0.0);
+        bool has_r = false;
+        std::vector<PTerm> T;                                   // thread / memory-bit terms
+        std::vector<std::pair<uint64_t, uint32_t>> S;           // mixed pi terms
+        struct G {
+            uint64_t cmem;
+            uint32_t cm;
+            cd p1;
+        };
+        std::vector<G> Gs;                                      // mixed general terms
+        auto add_t = [&](uint64_t cmem, cd p1, cd p0) {
+            for (PTerm& t : T)
+                if (t.mask == cmem) {
+                    t.p1 *= p1;
+                    t.p0 *= p0;
+                    return;
+                }
+            T.push_back({cmem, p1, p0});
+        };
+        for (const PTerm& t : pend_) {
+            if (is_one(t.p1) && is_one(t.p0)) continue;
+            uint32_t cm;
+            uint64_t cmem;
+            split_mask(pb, local_of, t.mask, cm, cmem);
+            if (cmem == 0) {
+                if (acc) {
+                    HostOp h = diag_host_op(cm, t.p1, t.p0);
+                    acc->cost += h.cost;
+                    acc->ops.push_back(std::move(h));
+                } else {
+                    for (uint32_t m = 0; m < 32; ++m) R[m] *= ((m & cm) == cm) ? t.p1 : t.p0;
+                    has_r = true;
+                }
+            } else if (cm == 0) {
+                add_t(cmem, t.p1, t.p0);
+            } else if (std::abs(t.p1 + cd(1.0, 0.0)) < 1e-12 && is_one(t.p0)) {
+                uint32_t pat = 0;
+                for (uint32_t m = 0; m < 32; ++m)
+                    if ((m & cm) == cm) pat |= 1u << m;
+                bool merged = false;
+                for (auto& sterm : S)
+                    if (sterm.first == cmem) {
+                        sterm.second ^= pat;
+                        merged = true;
+                        break;
+                    }
+                if (!merged) S.emplace_back(cmem, pat);
+            } else {
+                Gs.push_back({cmem, cm, t.p1});
+            }
+        }
+        pend_.clear();
+        pend_qubits_ = 0;
+        if (global) {
+            const double g = wrap_angle(pass_global_);
+            pass_global_ = 0.0;
+            if (g != 0.0) {
+                if (acc) {
+                    HostOp h = diag_host_op(0u, std::polar(1.0, g), cd(1.0, 0.0));
+                    acc->cost += h.cost;
+                    acc->ops.push_back(std::move(h));
+                } else {
+                    add_t(0, std::polar(1.0, g), std::polar(1.0, g));
+                }
+            }
+        }
+        if (has_r) {                                     // a flat table is a scalar
+            bool flat = true;
+            for (uint32_t m = 1; m < 32; ++m) flat = flat && std::abs(R[m] - R[0]) < 1e-15;
+            if (flat) {
+                if (!is_one(R[0])) add_t(0, R[0], R[0]);
+                has_r = false;
+            }
+        }
+        T.erase(std::remove_if(T.begin(), T.end(), [](const PTerm& t) { return is_one(t.p1) && is_one(t.p0); }),
+                T.end());
+        S.erase(std::remove_if(S.begin(), S.end(), [](const auto& x) { return x.second == 0u; }), S.end());
+        if (!has_r && T.empty() && S.empty() && Gs.empty()) return;
+        if (T.size() > 0xFFFF || S.size() > 0xFFFF) fail(QLB_ERR_INVALID_ARG, "too many diagonal terms in one pass");
+        auto f2 = [](cd z) { return make_float2(static_cast<float>(z.real()), static_cast<float>(z.imag())); };
+        auto words = [&](uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+            const uint32_t w[4] = {a, b, c, d};
+            float2 f[2];
+            std::memcpy(f, w, 16);
+            prog.mats.push_back(f[0]);
+            prog.mats.push_back(f[1]);
+        };
+        auto bits = [](float x) {
+            uint32_t u;
+            std::memcpy(&u, &x, 4);
+            return u;
+        };
+        if (prog.mats.size() & 1) prog.mats.push_back(make_float2(0.f, 0.f));
+        TileOp op{};
+        op.kind = TOP_DIAG;
+        op.code = OPC_DIAG;
+        op.data = static_cast<uint32_t>(prog.mats.size());
+        op.flags = has_r ? 1u : 0u;
+        op.n = static_cast<uint32_t>(T.size()) | (static_cast<uint32_t>(S.size()) << 16);
+        op.ctrl_reg = static_cast<uint32_t>(Gs.size());
+        if (has_r)
+            for (uint32_t m = 0; m < 32; ++m) prog.mats.push_back(f2(R[m]));
+        for (const PTerm& t : T) {
+            const float2 a = f2(t.p1), b = f2(t.p0);
+            words(static_cast<uint32_t>(t.mask), static_cast<uint32_t>(t.mask >> 32), bits(a.x), bits(a.y));
+            words(bits(b.x), bits(b.y), 0u, 0u);
+        }
+        for (const auto& x : S) words(static_cast<uint32_t>(x.first), static_cast<uint32_t>(x.first >> 32), x.second, 0u);
+        for (const G& g : Gs) {
+            const float2 a = f2(g.p1);
+            words(static_cast<uint32_t>(g.cmem), static_cast<uint32_t>(g.cmem >> 32), g.cm, 0u);
+            words(bits(a.x), bits(a.y), 0u, 0u);
+        }
+        prog.ops.push_back(op);
+    }
+
     void encode_ops(const PhaseBuild& pb, const TilePass&, const int* local_of, bool last_phase) {
         const bool tc = e_.mode == QLB_MODE_TILED_TC;
         Acc acc;
         for (uint32_t idx : pb.ops) {
-            for (HostOp& h : host_ops(pb, local_of, mi[idx])) {
+            const MI& m = mi[idx];
+            if (m.diag) {
+                double g = 0.0;
+                int singles = 0, others = 0;
+                for (const Term& t : m.terms) {
+                    if (t.a < 0) g += t.angle;
+                    else if (t.b < 0) ++singles;
+                    else ++others;
+                }
+                const bool fold = singles == 1 && others == 0;   // one qubit: the global part becomes p0
+                if (!fold) pass_global_ += g;
+                for (const Term& t : m.terms) {
+                    if (t.a < 0) continue;
+                    const uint64_t mask = bitm(static_cast<uint32_t>(t.a)) | (t.b >= 0 ? bitm(static_cast<uint32_t>(t.b)) : 0);
+                    const cd p1 = std::polar(1.0, wrap_angle(fold ? g + t.angle : t.angle));
+                    const cd p0 = fold ? std::polar(1.0, wrap_angle(g)) : cd(1.0, 0.0);
+                    if (tc) {
+                        uint32_t cm;
+                        uint64_t cmem;
+                        split_mask(pb, local_of, mask, cm, cmem);
+                        if (cmem == 0) {                 // register-only: straight into the accumulator
+                            HostOp h = diag_host_op(cm, p1, p0);
+                            acc.cost += h.cost;
+                            acc.ops.push_back(std::move(h));
+                            continue;
+                        }
+                        if (cm & acc.touched) flush(acc);
+                    }
+                    add_pending(mask, p1, p0);
+                }
+                continue;
+            }
+            if (pend_qubits_ & m.targets) flush_pending(pb, local_of, tc ? &acc : nullptr, false);
+            for (HostOp& h : host_ops(pb, local_of, m)) {
                 if (!tc) {
                     emit_cuda_op(h);
                     continue;
@@ -781,26 +962,14 @@ private:
                     acc.touched |= nondiag_bits(h);
                     acc.cost += h.cost;
                     acc.ops.push_back(std::move(h));
-                } else if (h.kind == TOP_CPHASE && (h.cm & acc.touched) == 0) {
-                    emit_cuda_op(h);                     // diagonal on untouched bits: commutes with acc
                 } else {
                     flush(acc);
                     emit_cuda_op(h);
                 }
             }
         }
+        if (last_phase) flush_pending(pb, local_of, tc ? &acc : nullptr, true);
         if (tc) flush(acc);
-        if (last_phase) {
-            const double g = wrap_angle(pass_global_);
-            if (g != 0.0) {
-                HostOp h;
-                h.kind = TOP_CPHASE;
-                h.m[0] = std::polar(1.0, g);
-                emit_cuda_op(h);
-            }
-            pass_global_ = 0.0;
-        }
-        flush_signs();
     }
 };
 
@@ -924,6 +1093,10 @@ std::string describe_plan_json(const PlanConfig& cfg, const qlb_gate_instr* prog
                 u(op.ctrl_mem);
                 out += ",\"flags\":";
                 u(op.flags);
+                out += ",\"n\":";
+                u(op.n);
+                out += ",\"code\":";
+                u(op.code);
                 out += ",\"data\":";
                 u(op.data);
                 out += ",\"m\":[";

@@ -159,10 +159,12 @@ __device__ __forceinline__ void u1_pair(float2& a0, float2& a1, const float2 (&m
     a0 = cfma(m[1], y, cmul(m[0], x));
     a1 = cfma(m[3], y, cmul(m[2], x));
 }
-__device__ __forceinline__ void u1r_pair(float2& a0, float2& a1, float m0, float m1, float m2, float m3) {
+// Real 2x2 with packed f32x2 arithmetic (both components per instruction);
+// m_i = (m_i, m_i).
+__device__ __forceinline__ void u1r_pair2(float2& a0, float2& a1, float2 m0, float2 m1, float2 m2, float2 m3) {
     const float2 x = a0, y = a1;
-    a0 = make_float2(fmaf(m1, y.x, m0 * x.x), fmaf(m1, y.y, m0 * x.y));
-    a1 = make_float2(fmaf(m3, y.x, m2 * x.x), fmaf(m3, y.y, m2 * x.y));
+    a0 = __ffma2_rn(m1, y, __fmul2_rn(m0, x));
+    a1 = __ffma2_rn(m3, y, __fmul2_rn(m2, x));
 }
 __device__ __forceinline__ void rx_pair(float2& a0, float2& a1, float c, float s) {
     const float2 x = a0, y = a1;
@@ -170,18 +172,18 @@ __device__ __forceinline__ void rx_pair(float2& a0, float2& a1, float c, float s
     a1 = make_float2(fmaf(s, x.y, c * y.x), fmaf(-s, x.x, c * y.y));
 }
 
-// Pair loops over register bit R; the common cm = 0 case has no predicates.
+// Pair loops over register bit R: uncontrolled, and under a register control mask.
 template <int R, typename F>
-__device__ __forceinline__ void for_pairs(float2 (&v)[NR], uint32_t cm, F&& f) {
-    if (cm == 0) {
+__device__ __forceinline__ void for_pairs(float2 (&v)[NR], F&& f) {
 #pragma unroll
-        for (int i = 0; i < NR; ++i)
-            if (!(i & (1 << R))) f(v[i], v[i | (1 << R)]);
-    } else {
+    for (int i = 0; i < NR; ++i)
+        if (!(i & (1 << R))) f(v[i], v[i | (1 << R)]);
+}
+template <int R, typename F>
+__device__ __forceinline__ void for_pairs_ctl(float2 (&v)[NR], uint32_t cm, F&& f) {
 #pragma unroll
-        for (int i = 0; i < NR; ++i)
-            if (!(i & (1 << R)) && ((static_cast<uint32_t>(i) & cm) == cm)) f(v[i], v[i | (1 << R)]);
-    }
+    for (int i = 0; i < NR; ++i)
+        if (!(i & (1 << R)) && ((static_cast<uint32_t>(i) & cm) == cm)) f(v[i], v[i | (1 << R)]);
 }
 
 template <int R0, int R1>
@@ -405,132 +407,164 @@ __device__ __forceinline__ bool op_dense_tc(float2 (&v)[NR], const float2* __res
     return true;
 }
 
-template <int CM>
-__device__ __forceinline__ void op_cphase(float2 (&v)[NR], float2 ph) {
+// TOP_DIAG: the per-thread factor of the thread/memory-bit terms, the sign
+// mask of the mixed pi terms, then one complex multiply per amplitude.
+__device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* __restrict__ tab, uint32_t has_r,
+                                        uint32_t n_t, uint32_t n_s, uint32_t n_g, uint64_t gt) {
+    const uint4* p = reinterpret_cast<const uint4*>(tab) + (has_r ? 16 : 0);
+    float2 T = make_float2(1.f, 0.f);
+#pragma unroll 2
+    for (uint32_t t = 0; t < n_t; ++t) {
+        const uint4 w0 = __ldg(p + 2 * t), w1 = __ldg(p + 2 * t + 1);
+        const uint64_t c = (static_cast<uint64_t>(w0.y) << 32) | w0.x;
+        const bool on = (gt & c) == c;
+        const float2 f = on ? make_float2(__uint_as_float(w0.z), __uint_as_float(w0.w))
+                            : make_float2(__uint_as_float(w1.x), __uint_as_float(w1.y));
+        T = cmul(T, f);
+    }
+    p += 2 * n_t;
+    uint32_t smask = 0;
+#pragma unroll 4
+    for (uint32_t t = 0; t < n_s; ++t) {
+        const uint4 w = __ldg(p + t);
+        const uint64_t c = (static_cast<uint64_t>(w.y) << 32) | w.x;
+        smask ^= ((gt & c) == c) ? w.z : 0u;
+    }
+    p += n_s;
+    if (has_r) {
 #pragma unroll
-    for (int i = 0; i < NR; ++i)
-        if ((i & CM) == CM) v[i] = cmul(v[i], ph);
-}
-template <int CM>
-__device__ __forceinline__ void op_negate(float2 (&v)[NR]) {
+        for (int m = 0; m < NR; ++m) v[m] = cmul(v[m], cmul(T, __ldg(tab + m)));
+    } else if (T.x != 1.f || T.y != 0.f) {
 #pragma unroll
-    for (int i = 0; i < NR; ++i)
-        if ((i & CM) == CM) v[i] = make_float2(-v[i].x, -v[i].y);
+        for (int m = 0; m < NR; ++m) v[m] = cmul(v[m], T);
+    }
+    if (smask) {
+#pragma unroll
+        for (int m = 0; m < NR; ++m) {
+            const uint32_t sgn = (smask << (31 - m)) & 0x80000000u;
+            v[m].x = __uint_as_float(__float_as_uint(v[m].x) ^ sgn);
+            v[m].y = __uint_as_float(__float_as_uint(v[m].y) ^ sgn);
+        }
+    }
+    for (uint32_t g = 0; g < n_g; ++g) {
+        const uint4 w0 = __ldg(p + 2 * g), w1 = __ldg(p + 2 * g + 1);
+        const uint64_t c = (static_cast<uint64_t>(w0.y) << 32) | w0.x;
+        if ((gt & c) != c) continue;
+        const uint32_t cm = w0.z;
+        const float2 ph = make_float2(__uint_as_float(w1.x), __uint_as_float(w1.y));
+#pragma unroll
+        for (int m = 0; m < NR; ++m)
+            if ((static_cast<uint32_t>(m) & cm) == cm) v[m] = cmul(v[m], ph);
+    }
 }
 
-#define QLB_R1(r, STMT)                                 \
-    switch (r) {                                        \
-    case 0: { constexpr int R = 0; STMT; } break;       \
-    case 1: { constexpr int R = 1; STMT; } break;       \
-    case 2: { constexpr int R = 2; STMT; } break;       \
-    case 3: { constexpr int R = 3; STMT; } break;       \
-    default: { constexpr int R = 4; STMT; } break;      \
-    }
+__device__ __forceinline__ float2 f2(uint32_t a, uint32_t b) { return make_float2(__uint_as_float(a), __uint_as_float(b)); }
 
-#define QLB_R2(a, b, STMT)                                              \
-    switch ((a) * 8 + (b)) {                                            \
-    case 0 * 8 + 1: { constexpr int A = 0, B = 1; STMT; } break;        \
-    case 0 * 8 + 2: { constexpr int A = 0, B = 2; STMT; } break;        \
-    case 0 * 8 + 3: { constexpr int A = 0, B = 3; STMT; } break;        \
-    case 0 * 8 + 4: { constexpr int A = 0, B = 4; STMT; } break;        \
-    case 1 * 8 + 2: { constexpr int A = 1, B = 2; STMT; } break;        \
-    case 1 * 8 + 3: { constexpr int A = 1, B = 3; STMT; } break;        \
-    case 1 * 8 + 4: { constexpr int A = 1, B = 4; STMT; } break;        \
-    case 2 * 8 + 3: { constexpr int A = 2, B = 3; STMT; } break;        \
-    case 2 * 8 + 4: { constexpr int A = 2, B = 4; STMT; } break;        \
-    default: { constexpr int A = 3, B = 4; STMT; } break;               \
-    }
-
-#define QLB_CASE_MASK(M, STMT) case M: { constexpr int CM = M; STMT; } break;
-#define QLB_MASK32(cm, STMT)                                                                       \
-    switch (cm) {                                                                                  \
-    QLB_CASE_MASK(0, STMT) QLB_CASE_MASK(1, STMT) QLB_CASE_MASK(2, STMT) QLB_CASE_MASK(3, STMT)     \
-    QLB_CASE_MASK(4, STMT) QLB_CASE_MASK(5, STMT) QLB_CASE_MASK(6, STMT) QLB_CASE_MASK(7, STMT)     \
-    QLB_CASE_MASK(8, STMT) QLB_CASE_MASK(9, STMT) QLB_CASE_MASK(10, STMT) QLB_CASE_MASK(11, STMT)   \
-    QLB_CASE_MASK(12, STMT) QLB_CASE_MASK(13, STMT) QLB_CASE_MASK(14, STMT) QLB_CASE_MASK(15, STMT) \
-    QLB_CASE_MASK(16, STMT) QLB_CASE_MASK(17, STMT) QLB_CASE_MASK(18, STMT) QLB_CASE_MASK(19, STMT) \
-    QLB_CASE_MASK(20, STMT) QLB_CASE_MASK(21, STMT) QLB_CASE_MASK(22, STMT) QLB_CASE_MASK(23, STMT) \
-    QLB_CASE_MASK(24, STMT) QLB_CASE_MASK(25, STMT) QLB_CASE_MASK(26, STMT) QLB_CASE_MASK(27, STMT) \
-    QLB_CASE_MASK(28, STMT) QLB_CASE_MASK(29, STMT) QLB_CASE_MASK(30, STMT)                         \
-    default: { constexpr int CM = 31; STMT; } break;                                               \
-    }
-
+// The op loop of one phase.  Each op is four 16-byte words; the first holds
+// the dispatch code, the register controls and the data offset.
 __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, const TileOp* ops,
                                         const float2* __restrict__ mats, float2* sm, const PhaseMap& M,
                                         bool linear, TcCtx& tc) {
+    const uint4* rec = reinterpret_cast<const uint4*>(ops);
     for (uint32_t oi = ph.op_begin; oi < ph.op_end; ++oi) {
-        const TileOp& op = ops[oi];
-        if (op.kind == TOP_DENSE_TC) {      // CTA-wide; never controlled
-            if (!op_dense_tc(v, mats + op.data, sm, tc)) return false;
-            continue;
+        const uint4 q0 = rec[4 * oi];
+        if (q0.y & 0x00FF0000u) {          // memory controls: a thread-uniform condition
+            const uint4 q1 = rec[4 * oi + 1];
+            const uint64_t c = (static_cast<uint64_t>(q1.w) << 32) | q1.z;
+            if ((M.gt & c) != c) continue;
         }
-        if ((M.gt & op.ctrl_mem) != op.ctrl_mem) continue;   // thread-uniform condition
-        const uint32_t cm = op.ctrl_reg;
-        switch (op.kind) {
-        case TOP_SIGNS: {
-            // per-thread negate mask over the 32 registers, then sign-bit XORs
-            const uint4* terms = reinterpret_cast<const uint4*>(mats + op.data);
-            uint32_t mask = 0;
-            for (uint32_t t = 0; t < op.flags; ++t) {
-                const uint4 w = __ldg(terms + t);
-                const uint64_t cmem = (static_cast<uint64_t>(w.y) << 32) | w.x;
-                mask ^= ((M.gt & cmem) == cmem) ? w.z : 0u;
-            }
+        const uint32_t cm = q0.z, data = q0.w;
+        switch (q0.x & 0xFFFFu) {
+#define QLB_U1R_CASE(RR)                                                                              \
+    case OPC_U1R + RR: {                                                                              \
+        const uint4 a = rec[4 * oi + 2], b = rec[4 * oi + 3];                                         \
+        const float2 m0 = f2(a.x, a.x), m1 = f2(a.z, a.z), m2 = f2(b.x, b.x), m3 = f2(b.z, b.z);      \
+        for_pairs<RR>(v, [&](float2& x, float2& y) { u1r_pair2(x, y, m0, m1, m2, m3); });             \
+    } break;
+#define QLB_RX_CASE(RR)                                                                               \
+    case OPC_RX + RR: {                                                                               \
+        const uint4 a = rec[4 * oi + 2];                                                              \
+        const float c = __uint_as_float(a.x), s = __uint_as_float(a.y);                               \
+        for_pairs<RR>(v, [&](float2& x, float2& y) { rx_pair(x, y, c, s); });                         \
+    } break;
+#define QLB_U1_CASE(RR)                                                                               \
+    case OPC_U1 + RR: {                                                                               \
+        const uint4 a = rec[4 * oi + 2], b = rec[4 * oi + 3];                                         \
+        const float2 m[4] = {f2(a.x, a.y), f2(a.z, a.w), f2(b.x, b.y), f2(b.z, b.w)};                 \
+        for_pairs<RR>(v, [&](float2& x, float2& y) { u1_pair(x, y, m); });                            \
+    } break;                                                                                          \
+    case OPC_U1_CTL + RR: {                                                                           \
+        const uint4 a = rec[4 * oi + 2], b = rec[4 * oi + 3];                                         \
+        const float2 m[4] = {f2(a.x, a.y), f2(a.z, a.w), f2(b.x, b.y), f2(b.z, b.w)};                 \
+        for_pairs_ctl<RR>(v, cm, [&](float2& x, float2& y) { u1_pair(x, y, m); });                    \
+    } break;
+#define QLB_X_CASE(RR)                                                                                \
+    case OPC_X + RR:                                                                                  \
+        for_pairs<RR>(v, [](float2& x, float2& y) { const float2 t = x; x = y; y = t; });             \
+        break;                                                                                        \
+    case OPC_X_CTL + RR:                                                                              \
+        for_pairs_ctl<RR>(v, cm, [](float2& x, float2& y) { const float2 t = x; x = y; y = t; });     \
+        break;
+#define QLB_PAIR_CASES(A, B)                                                                          \
+    case OPC_SWAP + reg_pair_index(A, B): op_swap<A, B>(v, cm); break;                                \
+    case OPC_U2 + reg_pair_index(A, B): op_u2<A, B>(v, mats + data, cm); break;
+            QLB_U1R_CASE(0) QLB_U1R_CASE(1) QLB_U1R_CASE(2) QLB_U1R_CASE(3) QLB_U1R_CASE(4)
+            QLB_RX_CASE(0) QLB_RX_CASE(1) QLB_RX_CASE(2) QLB_RX_CASE(3) QLB_RX_CASE(4)
+            QLB_U1_CASE(0) QLB_U1_CASE(1) QLB_U1_CASE(2) QLB_U1_CASE(3) QLB_U1_CASE(4)
+            QLB_X_CASE(0) QLB_X_CASE(1) QLB_X_CASE(2) QLB_X_CASE(3) QLB_X_CASE(4)
+            QLB_PAIR_CASES(0, 1) QLB_PAIR_CASES(0, 2) QLB_PAIR_CASES(0, 3) QLB_PAIR_CASES(0, 4)
+            QLB_PAIR_CASES(1, 2) QLB_PAIR_CASES(1, 3) QLB_PAIR_CASES(1, 4)
+            QLB_PAIR_CASES(2, 3) QLB_PAIR_CASES(2, 4) QLB_PAIR_CASES(3, 4)
+#undef QLB_U1R_CASE
+#undef QLB_RX_CASE
+#undef QLB_U1_CASE
+#undef QLB_X_CASE
+#undef QLB_PAIR_CASES
+        case OPC_DENSE3: op_dense_reg<3>(v, mats + data); break;
+        case OPC_DENSE4: op_dense_reg<4>(v, mats + data); break;
+        case OPC_DENSE5: op_dense5(v, mats + data, sm, M, linear); break;
+        case OPC_DENSE_TC:                 // CTA-wide; never controlled
+            if (!op_dense_tc(v, mats + data, sm, tc)) return false;
+            break;
+        case OPC_DIAG: {
+            const uint4 q1 = rec[4 * oi + 1];
+            op_diag(v, mats + data, q1.x & 1u, q1.y & 0xFFFFu, q1.y >> 16, cm, M.gt);
+            break;
+        }
+        case OPC_CPHASE: {
+            const uint4 a = rec[4 * oi + 2];
+            const float2 p = f2(a.x, a.y);
 #pragma unroll
-            for (int m = 0; m < NR; ++m) {
-                const uint32_t sgn = (mask << (31 - m)) & 0x80000000u;
-                v[m].x = __uint_as_float(__float_as_uint(v[m].x) ^ sgn);
-                v[m].y = __uint_as_float(__float_as_uint(v[m].y) ^ sgn);
-            }
+            for (int i = 0; i < NR; ++i)
+                if ((static_cast<uint32_t>(i) & cm) == cm) v[i] = cmul(v[i], p);
             break;
         }
-        case TOP_CPHASE:
-            if (op.flags & 1u) {
-                QLB_MASK32(cm, op_negate<CM>(v));
-            } else {
-                const float2 p = op.m[0];
-                QLB_MASK32(cm, op_cphase<CM>(v, p));
-            }
-            break;
-        case TOP_U1: {
-            const float2 m[4] = {op.m[0], op.m[1], op.m[2], op.m[3]};
-            QLB_R1(op.r0, for_pairs<R>(v, cm, [&](float2& a, float2& b) { u1_pair(a, b, m); }));
-            break;
-        }
-        case TOP_U1R: {
-            const float m0 = op.m[0].x, m1 = op.m[1].x, m2 = op.m[2].x, m3 = op.m[3].x;
-            QLB_R1(op.r0, for_pairs<R>(v, cm, [&](float2& a, float2& b) { u1r_pair(a, b, m0, m1, m2, m3); }));
-            break;
-        }
-        case TOP_RX: {
-            const float c = op.m[0].x, s = op.m[0].y;
-            QLB_R1(op.r0, for_pairs<R>(v, cm, [&](float2& a, float2& b) { rx_pair(a, b, c, s); }));
-            break;
-        }
-        case TOP_X:
-            QLB_R1(op.r0, for_pairs<R>(v, cm, [](float2& a, float2& b) {
-                const float2 t = a;
-                a = b;
-                b = t;
-            }));
-            break;
-        case TOP_SWAP: QLB_R2(op.r0, op.r1, (op_swap<A, B>(v, cm))); break;
-        case TOP_U2: QLB_R2(op.r0, op.r1, (op_u2<A, B>(v, mats + op.data, cm))); break;
-        case TOP_DENSE:
-            if (op.k == 3) op_dense_reg<3>(v, mats + op.data);
-            else if (op.k == 4) op_dense_reg<4>(v, mats + op.data);
-            else op_dense5(v, mats + op.data, sm, M, linear);
-            break;
         default: break;
         }
     }
     return true;
 }
 
+// Largest i with work[i].tile_begin <= tile (entries sorted by tile_begin).
+__device__ __forceinline__ uint32_t find_work(const TileWork* __restrict__ work, uint32_t n_work, uint64_t tile) {
+    uint32_t lo = 0, hi = n_work;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (work[mid].tile_begin <= tile) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// One launch applies one pass to each entry of a work list: the launch's
+// flattened tile range is the concatenation of the entries' tiles (a single
+// state: one entry passed by value, n_work = 0).  A CTA restages the pass
+// descriptor, phases and ops in shared memory when its next tile belongs to
+// a different pass.
 __global__ void __launch_bounds__(NT, 1)
-k_tile_pass(float2* __restrict__ state, const TilePass* __restrict__ passes, const TilePhase* __restrict__ gphases,
-            const TileOp* __restrict__ gops, const float2* __restrict__ mats, uint32_t pass_index,
-            uint64_t ntiles, int has_tc, int* __restrict__ err) {
+k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work, uint64_t ntiles,
+            const TilePass* __restrict__ passes, const TilePhase* __restrict__ gphases,
+            const TileOp* __restrict__ gops, const float2* __restrict__ mats, int has_tc, int* __restrict__ err) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     float2* bufs = reinterpret_cast<float2*>(smem_raw);
     TileOp* sops = reinterpret_cast<TileOp*>(smem_raw + kSmemBuffers);
@@ -540,27 +574,6 @@ k_tile_pass(float2* __restrict__ state, const TilePass* __restrict__ passes, con
     uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(bar + 3);
     unsigned char* sb = smem_raw + kSmemBuffers + kSmemOps + kSmemPhases + sizeof(TilePass) + kSmemMisc;
 
-    const TilePass& GP = passes[pass_index];
-    // Stage the pass descriptor, its phases and (if they fit) its ops.
-    {
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(&GP);
-        uint32_t* dst = reinterpret_cast<uint32_t*>(spass);
-        for (uint32_t i = threadIdx.x; i < sizeof(TilePass) / 4; i += NT) dst[i] = src[i];
-    }
-    const uint32_t pb = GP.phase_begin, pe = GP.phase_end;
-    const uint32_t nph = pe - pb;
-    const bool ph_in_smem = nph <= kMaxSmemPhases;
-    if (ph_in_smem)
-        for (uint32_t i = threadIdx.x; i < nph * sizeof(TilePhase) / 4; i += NT)
-            reinterpret_cast<uint32_t*>(sph)[i] = reinterpret_cast<const uint32_t*>(gphases + pb)[i];
-    const uint32_t ob = gphases[pb].op_begin, oe = gphases[pe - 1].op_end;
-    const bool ops_in_smem = (oe - ob) <= kMaxSmemOps;
-    if (ops_in_smem)
-        for (uint32_t i = threadIdx.x; i < (oe - ob) * sizeof(TileOp) / 4; i += NT)
-            reinterpret_cast<uint32_t*>(sops)[i] = reinterpret_cast<const uint32_t*>(gops + ob)[i];
-    // phase op ranges index the global op array; rebase the shared copy
-    const TilePhase* phases = ph_in_smem ? sph : gphases + pb;
-    const TileOp* ops = ops_in_smem ? sops - ob : gops;
     if (threadIdx.x == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
@@ -576,22 +589,62 @@ k_tile_pass(float2* __restrict__ state, const TilePass* __restrict__ passes, con
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const TilePass& P = *spass;
     TcCtx tc{has_tc ? *tmem_holder : 0u, &bar[2], sb, 0u};
     bool failed = false;
 
+    auto entry = [&](uint64_t t) -> TileWork { return n_work ? work[find_work(work, n_work, t)] : single; };
+
+    // Stage pass `pi`: its descriptor, phases and (if they fit) ops.  Phase
+    // op ranges index the global op array; the shared copy is rebased.
+    uint32_t staged = ~0u, nph = 0;
+    const TilePhase* phases = nullptr;
+    const TileOp* ops = nullptr;
+    auto stage = [&](uint32_t pi) {
+        const TilePass& GP = passes[pi];
+        {
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(&GP);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(spass);
+            for (uint32_t i = threadIdx.x; i < sizeof(TilePass) / 4; i += NT) dst[i] = src[i];
+        }
+        const uint32_t pb = GP.phase_begin, pe = GP.phase_end;
+        nph = pe - pb;
+        const bool ph_in_smem = nph <= kMaxSmemPhases;
+        if (ph_in_smem)
+            for (uint32_t i = threadIdx.x; i < nph * sizeof(TilePhase) / 4; i += NT)
+                reinterpret_cast<uint32_t*>(sph)[i] = reinterpret_cast<const uint32_t*>(gphases + pb)[i];
+        const uint32_t ob = gphases[pb].op_begin, oe = gphases[pe - 1].op_end;
+        const bool ops_in_smem = (oe - ob) <= kMaxSmemOps;
+        if (ops_in_smem)
+            for (uint32_t i = threadIdx.x; i < (oe - ob) * sizeof(TileOp) / 16; i += NT)
+                reinterpret_cast<uint4*>(sops)[i] = reinterpret_cast<const uint4*>(gops + ob)[i];
+        phases = ph_in_smem ? sph : gphases + pb;
+        ops = ops_in_smem ? sops - ob : gops;
+        staged = pi;
+    };
+
     uint64_t tile = blockIdx.x;
     float2* xbuf = bufs + 2 * static_cast<size_t>(TILE);
-    if (tile < ntiles) issue_tile_load(bufs, state, P, tile, &bar[0]);
+    if (tile < ntiles) {
+        const TileWork w = entry(tile);
+        issue_tile_load(bufs, w.state, passes[w.pass], tile - w.tile_begin, &bar[0]);
+    }
     uint32_t it = 0;
     for (; tile < ntiles; tile += gridDim.x, ++it) {
+        const TileWork w = entry(tile);
+        if (w.pass != staged) {          // uniform: every thread reads the same entry
+            __syncthreads();
+            stage(w.pass);
+            __syncthreads();
+        }
+        const TilePass& P = *spass;
         const uint32_t b = it & 1u;
         float2* cur = bufs + static_cast<size_t>(b) * TILE;
         float2* nxt = bufs + static_cast<size_t>(b ^ 1u) * TILE;
         const uint64_t next = tile + gridDim.x;
         if (next < ntiles) {
+            const TileWork wn = entry(next);
             fence_proxy_async();   // earlier generic-proxy reads of nxt precede the async-proxy writes
-            issue_tile_load(nxt, state, P, next, &bar[b ^ 1u]);
+            issue_tile_load(nxt, wn.state, passes[wn.pass], next - wn.tile_begin, &bar[b ^ 1u]);
         }
         const bool ok = mbar_wait_bounded(&bar[b], (it >> 1) & 1u);
         if (__syncthreads_or(!ok)) {
@@ -600,7 +653,8 @@ k_tile_pass(float2* __restrict__ state, const TilePass* __restrict__ passes, con
             failed = true;
             break;
         }
-        const uint64_t base = tile_base(P, tile);
+        float2* __restrict__ state = w.state;
+        const uint64_t base = tile_base(P, tile - w.tile_begin);
         float2 v[NR];
         PhaseMap M = make_map(P, phases[0], base);
 #pragma unroll
@@ -653,9 +707,8 @@ k_tile_pass(float2* __restrict__ state, const TilePass* __restrict__ passes, con
 
 }  // namespace
 
-cudaError_t launch_tile_pass(float2* state, uint32_t n, const TilePass* d_passes, const TilePhase* d_phases,
-                             const TileOp* d_ops, const float2* d_mats, uint32_t pass_index, int has_tc,
-                             int* err, cudaStream_t s) {
+namespace {
+cudaError_t configure_tile_kernel() {
     static bool configured = false;
     if (!configured) {
         cudaError_t e = cudaFuncSetAttribute(k_tile_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -663,11 +716,35 @@ cudaError_t launch_tile_pass(float2* state, uint32_t n, const TilePass* d_passes
         if (e != cudaSuccess) return e;
         configured = true;
     }
+    return cudaSuccess;
+}
+}  // namespace
+
+cudaError_t launch_tile_pass(float2* state, uint32_t n, const TilePass* d_passes, const TilePhase* d_phases,
+                             const TileOp* d_ops, const float2* d_mats, uint32_t pass_index, int has_tc,
+                             int* err, cudaStream_t s) {
+    cudaError_t e = configure_tile_kernel();
+    if (e != cudaSuccess) return e;
     const uint64_t tiles = uint64_t{1} << (n - kTileQubits);
     uint64_t grid = static_cast<uint64_t>(sm_count());
     if (grid > tiles) grid = tiles;
-    k_tile_pass<<<static_cast<unsigned>(grid), NT, kSmemTotal, s>>>(state, d_passes, d_phases, d_ops, d_mats,
-                                                                     pass_index, tiles, has_tc, err);
+    const TileWork single{state, 0, pass_index, 0};
+    k_tile_pass<<<static_cast<unsigned>(grid), NT, kSmemTotal, s>>>(single, nullptr, 0, tiles, d_passes, d_phases,
+                                                                     d_ops, d_mats, has_tc, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tile_work(const TileWork* d_work, uint32_t n_work, uint64_t total_tiles, const TilePass* d_passes,
+                             const TilePhase* d_phases, const TileOp* d_ops, const float2* d_mats, int has_tc,
+                             int* err, cudaStream_t s) {
+    if (n_work == 0 || total_tiles == 0) return cudaSuccess;
+    cudaError_t e = configure_tile_kernel();
+    if (e != cudaSuccess) return e;
+    uint64_t grid = static_cast<uint64_t>(sm_count());
+    if (grid > total_tiles) grid = total_tiles;
+    const TileWork none{nullptr, 0, 0, 0};
+    k_tile_pass<<<static_cast<unsigned>(grid), NT, kSmemTotal, s>>>(none, d_work, n_work, total_tiles, d_passes,
+                                                                     d_phases, d_ops, d_mats, has_tc, err);
     return cudaGetLastError();
 }
 

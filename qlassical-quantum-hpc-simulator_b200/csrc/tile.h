@@ -46,20 +46,54 @@ enum TileOpKind : uint8_t {
     TOP_DENSE = 5,    // 2^k x 2^k on register bits 0..k-1 (k = 3..5), FP32
     TOP_U1R = 6,      // real 2x2 (m[i].x) on register bit r0 (H, RY)
     TOP_RX = 7,       // [[c, -is], [-is, c]] on r0, c = m[0].x, s = m[0].y
-    TOP_CPHASE = 8,   // amplitudes with ctrl_reg/ctrl_mem bits all set *= m[0]; flags&1: m[0] == -1
+    TOP_CPHASE = 8,   // amplitudes with ctrl_reg/ctrl_mem bits all set *= m[0]
     TOP_DENSE_TC = 9, // k = 5 on register bits 0..4 on the tensor cores
-    TOP_SIGNS = 10    // a run of pi phases: flags terms {u64 ctrl_mem, u32 register pattern} at data
+    TOP_DIAG = 11     // a run of diagonal gates: one phase factor per amplitude (layout below)
 };
 
+// Device dispatch codes: one handler per (kind, register bit / bit pair,
+// controlled or not), so the kernel's op loop is a single jump table.
+enum TileOpCode : uint16_t {
+    OPC_NOP = 0,
+    OPC_U1 = 1,          // + r0, uncontrolled
+    OPC_U1R = 6,         // + r0
+    OPC_RX = 11,         // + r0
+    OPC_X = 16,          // + r0
+    OPC_U1_CTL = 21,     // + r0, register controls ctrl_reg (any 1-qubit kind, complex m)
+    OPC_X_CTL = 26,      // + r0
+    OPC_SWAP = 31,       // + pair index of (r0 < r1)
+    OPC_U2 = 41,         // + pair index
+    OPC_DENSE3 = 51,
+    OPC_DENSE4 = 52,
+    OPC_DENSE5 = 53,
+    OPC_DENSE_TC = 54,
+    OPC_DIAG = 55,
+    OPC_CPHASE = 56,
+    OPC_COUNT = 57
+};
+// (a, b), a < b < 5  ->  0..9
+__host__ __device__ constexpr uint32_t reg_pair_index(uint32_t a, uint32_t b) { return a * (9u - a) / 2u + (b - a - 1u); }
+
+// One register-level op, 64 bytes (four 16-byte words read with vector loads).
+//   TOP_DIAG: data = float2 offset of its tables in the matrix buffer:
+//     [flags & 1] R: 32 float2, the factor of each register index (terms on register bits only)
+//     n & 0xFFFF  T terms, 32 B each: {u64 mem mask, float2 p1, float2 p0}: a thread whose
+//                 index has every mask bit set multiplies by p1, otherwise by p0
+//     n >> 16     S terms, 16 B each: {u64 mem mask, u32 register pattern, 0}: sign flips
+//     ctrl_reg    G terms, 32 B each: {u64 mem mask, u32 register mask, 0, float2 phase, 0, 0}
 struct TileOp {
-    uint8_t kind;
-    uint8_t r0, r1, k;
+    uint16_t code;          // TileOpCode
+    uint8_t kind, k;        // TileOpKind; DENSE: k
+    uint8_t r0, r1;
+    uint8_t has_mem, pad;   // has_mem: ctrl_mem != 0
     uint32_t ctrl_reg;      // register-bit mask that must be all ones
+    uint32_t data;          // U2/DENSE/TC/DIAG: float2 offset into the matrix buffer
+    uint32_t flags;
+    uint32_t n;
     uint64_t ctrl_mem;      // memory-qubit mask (non-register qubits) that must be all ones
     float2 m[4];            // matrix / coefficients / phase
-    uint32_t data;          // TOP_U2/DENSE: float2 offset of the matrix
-    uint32_t flags;
 };
+static_assert(sizeof(TileOp) == 64, "TileOp is four 16-byte words");
 
 struct TilePhase {
     uint8_t reg_pos[kRegQubits];      // register bit j <- tile-local position
@@ -85,10 +119,24 @@ struct TileProgram {
     std::vector<float2> mats;
 };
 
+// One entry of a multi-state launch: tiles [tile_begin, tile_begin +
+// 2^(n - 13)) of the launch's flattened tile range apply pass `pass` to the
+// state at `state` (entries sorted by tile_begin, contiguous).
+struct TileWork {
+    float2* state;
+    uint64_t tile_begin;
+    uint32_t pass;
+    uint32_t pad;
+};
+
 // `err` (device int) receives a nonzero code if a bounded wait gave up.
 // `has_tc`: the pass contains TOP_DENSE_TC ops (the CTA allocates tensor memory).
 cudaError_t launch_tile_pass(float2* state, uint32_t n, const TilePass* d_passes, const TilePhase* d_phases,
                              const TileOp* d_ops, const float2* d_mats, uint32_t pass_index, int has_tc,
+                             int* err, cudaStream_t s);
+// One launch over a work list in device memory (batched and served states).
+cudaError_t launch_tile_work(const TileWork* d_work, uint32_t n_work, uint64_t total_tiles, const TilePass* d_passes,
+                             const TilePhase* d_phases, const TileOp* d_ops, const float2* d_mats, int has_tc,
                              int* err, cudaStream_t s);
 
 // Host-side helpers shared between engine.cpp and tile.cpp.

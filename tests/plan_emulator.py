@@ -8,7 +8,8 @@ from __future__ import annotations
 
 import numpy as np
 
-TOP_U1, TOP_X, TOP_SWAP, TOP_U2, TOP_DENSE, TOP_U1R, TOP_RX, TOP_CPHASE, TOP_DENSE_TC, TOP_SIGNS = range(1, 11)
+TOP_U1, TOP_X, TOP_SWAP, TOP_U2, TOP_DENSE, TOP_U1R, TOP_RX, TOP_CPHASE, TOP_DENSE_TC = range(1, 10)
+TOP_DIAG = 11
 STEP_PASS, STEP_PLAIN, STEP_MEASURE, STEP_SWAP = range(4)
 
 
@@ -73,23 +74,12 @@ def emulate(plan, init=None):
                         apply_k(st, n, mq[:k], mats[op["data"]:op["data"] + D * D].reshape(D, D), cmask)
                     elif kd == TOP_DENSE_TC:
                         apply_k(st, n, mq[:5], decode_tc_flat(plan, op["data"]), 0)
-                    elif kd == TOP_SIGNS:
-                        w = words[2 * op["data"]:2 * op["data"] + 4 * op["flags"]].reshape(-1, 4)
-                        idx = np.arange(1 << n, dtype=np.int64)
-                        reg = np.zeros(idx.shape, dtype=np.int64)
-                        for j in range(5):
-                            reg |= ((idx >> mq[j]) & 1) << j
-                        flip = np.zeros(idx.shape, dtype=bool)
-                        for t in w:
-                            cmem = int(t[0]) | (int(t[1]) << 32)
-                            pat = int(t[2])
-                            hit = ((idx & cmem) == cmem) & (((pat >> reg) & 1) == 1)
-                            flip ^= hit
-                        st[flip] *= -1.0
+                    elif kd == TOP_DIAG:
+                        apply_diag(st, n, mq, op, words)
                     elif kd == TOP_CPHASE:
                         idx = np.arange(1 << n, dtype=np.int64)
                         sel = (idx & cmask) == cmask
-                        st[sel] *= (-1.0 if op["flags"] & 1 else mc[0])
+                        st[sel] *= mc[0]
                     else:
                         raise ValueError(f"unknown op kind {kd}")
         elif kind == STEP_PLAIN:
@@ -107,6 +97,45 @@ def emulate(plan, init=None):
         else:
             raise ValueError("MEASURE steps are not emulated")
     return st
+
+
+def apply_diag(st, n, mq, op, words):
+    """TOP_DIAG: R table over the register index, T terms (thread/memory
+    masks, p1 where all set else p0), S sign terms, G general mixed terms."""
+    idx = np.arange(1 << n, dtype=np.int64)
+    reg = np.zeros(idx.shape, dtype=np.int64)
+    for j in range(5):
+        reg |= ((idx >> mq[j]) & 1) << j
+    w = words[2 * op["data"]:].astype(np.uint64)
+    f = words[2 * op["data"]:].view(np.float32).astype(np.float64)
+    pos = 0
+    fac = np.ones(idx.shape, dtype=np.complex128)
+    if op["flags"] & 1:
+        R = f[0:64:2] + 1j * f[1:64:2]
+        fac *= R[reg]
+        pos = 64
+    n_t, n_s, n_g = op["n"] & 0xFFFF, op["n"] >> 16, op["ctrl_reg"]
+    for _ in range(n_t):
+        c = int(w[pos]) | (int(w[pos + 1]) << 32)
+        p1 = f[pos + 2] + 1j * f[pos + 3]
+        p0 = f[pos + 4] + 1j * f[pos + 5]
+        on = (idx & c) == c
+        fac *= np.where(on, p1, p0)
+        pos += 8
+    for _ in range(n_s):
+        c = int(w[pos]) | (int(w[pos + 1]) << 32)
+        pat = int(w[pos + 2])
+        hit = ((idx & c) == c) & (((pat >> reg) & 1) == 1)
+        fac[hit] *= -1.0
+        pos += 4
+    for _ in range(n_g):
+        c = int(w[pos]) | (int(w[pos + 1]) << 32)
+        cm = int(w[pos + 2])
+        ph = f[pos + 4] + 1j * f[pos + 5]
+        hit = ((idx & c) == c) & ((reg & cm) == cm)
+        fac[hit] *= ph
+        pos += 8
+    st *= fac
 
 
 _tc_cache = {}
