@@ -157,8 +157,11 @@ int qlb_engine_get_mode(qlb_engine_t e, int* mode);
  * data (one bandwidth-bound swap pass each, logical order restored when
  * execute() returns); 0 (default) applies the permutation lazily by
  * re-addressing later instructions, which gives the same state with no
- * data movement. */
-enum qlb_option { QLB_OPT_PHYSICAL_GLOBAL_SWAP = 1 };
+ * data movement.  QLB_OPT_TC_MIN_COST (TILED_TC only): a run of
+ * register-local ops goes to the tensor cores when its estimated CUDA-core
+ * cost, in hundredths of an instruction per amplitude, reaches the value
+ * (default 1000); cheaper runs stay on the CUDA cores. */
+enum qlb_option { QLB_OPT_PHYSICAL_GLOBAL_SWAP = 1, QLB_OPT_TC_MIN_COST = 2 };
 int qlb_engine_set_option(qlb_engine_t e, int key, int64_t value);
 int qlb_engine_synchronize(qlb_engine_t e);
 /* The device state pointer (float2 *) and the stream the engine launches on. */
@@ -255,6 +258,47 @@ int qlb_module_program(qlb_module_t m, const qlb_gate_instr** program, uint64_t*
 int qlb_module_pool(qlb_module_t m, qlb_pool_view* out);
 /* GPUTopology::get_safe_qubit_limit(): the shared-memory tile window. */
 int qlb_gpu_safe_qubit_limit(uint32_t* out);
+
+/* ------------------------------------------------------------------------ */
+/* Batched mode: many independent circuits per launch.  No counterpart in   */
+/* the reference (its engine runs one circuit per CPUOpenMPEngine); the     */
+/* per-circuit semantics are execute() on |0...0> followed by <Z_i>.        */
+/* ------------------------------------------------------------------------ */
+
+typedef struct qlb_batch* qlb_batch_t;
+
+typedef struct qlb_batch_info {
+    uint32_t circuits;
+    uint32_t rounds;        /* tile-kernel launches = max passes over the circuits */
+    int      mode;          /* the mode in use (the autotuner's pick for mode -1) */
+    uint32_t launches;      /* kernel launches per run */
+    uint64_t tiles;         /* 2^13-amplitude tiles processed per run */
+    uint64_t passes;        /* sum over circuits of executed passes */
+    uint64_t amp_updates;   /* sum over circuits of (gates * 2^num_qubits) */
+    uint64_t state_bytes;   /* device bytes of all state vectors */
+    double   autotune_ms[2];/* mode -1: one run with TILED, with TILED_TC */
+} qlb_batch_info;
+
+/* Plans `count` circuits (program c: counts[c] instructions over pools[c],
+ * num_qubits[c] in 1..30; gates only -- no MEASURE or 6-qubit blocks),
+ * allocates every state vector and captures one CUDA graph per run.
+ * mode: QLB_MODE_TILED, QLB_MODE_TILED_TC, or -1 to time both and keep the
+ * faster. */
+int qlb_batch_create(qlb_batch_t* out, uint32_t count, const qlb_gate_instr* const* programs,
+                     const uint64_t* counts, const qlb_pool_view* pools, const uint32_t* num_qubits,
+                     int mode);
+/* Resets every state to |0...0>, runs all circuits and the FP64 <Z_i>
+ * reductions: one graph launch on the batch's stream (asynchronous). */
+int qlb_batch_run(qlb_batch_t b);
+/* Waits for the run; QLB_ERR_TIMEOUT if a bounded device wait gave up. */
+int qlb_batch_synchronize(qlb_batch_t b);
+/* <Z_q> of circuit c into out[c * stride + q], q < num_qubits[c]. */
+int qlb_batch_expect_z(qlb_batch_t b, double* out, uint32_t stride);
+/* Amplitudes of circuit `index` (complex128, dim = 2^num_qubits). */
+int qlb_batch_state(qlb_batch_t b, uint32_t index, double* out_c128, uint64_t dim);
+int qlb_batch_stats(qlb_batch_t b, qlb_batch_info* out);
+int qlb_batch_stream(qlb_batch_t b, void** out_cuda_stream);
+int qlb_batch_destroy(qlb_batch_t b);
 
 #ifdef __cplusplus
 }

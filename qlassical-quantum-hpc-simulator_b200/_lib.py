@@ -88,6 +88,20 @@ class ExecStats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class BatchInfo(ctypes.Structure):
+    _fields_ = [
+        ("circuits", ctypes.c_uint32),
+        ("rounds", ctypes.c_uint32),
+        ("mode", ctypes.c_int),
+        ("launches", ctypes.c_uint32),
+        ("tiles", ctypes.c_uint64),
+        ("passes", ctypes.c_uint64),
+        ("amp_updates", ctypes.c_uint64),
+        ("state_bytes", ctypes.c_uint64),
+        ("autotune_ms", ctypes.c_double * 2),
+    ]
+
+
 class TranspileConfig(ctypes.Structure):
     _fields_ = [
         ("enable_gate_fusion", ctypes.c_int),
@@ -151,6 +165,14 @@ _SIGNATURES = {
     "qlb_engine_run": [_P, _P],
     "qlb_plan_stats": [_P, ctypes.POINTER(ExecStats)],
     "qlb_plan_destroy": [_P],
+    "qlb_batch_create": [ctypes.POINTER(_P), _U32, _P, _P, _P, _P, _I],
+    "qlb_batch_run": [_P],
+    "qlb_batch_synchronize": [_P],
+    "qlb_batch_expect_z": [_P, _P, _U32],
+    "qlb_batch_state": [_P, _U32, _P, _U64],
+    "qlb_batch_stats": [_P, ctypes.POINTER(BatchInfo)],
+    "qlb_batch_stream": [_P, ctypes.POINTER(_P)],
+    "qlb_batch_destroy": [_P],
 }
 _OPTIONAL = {
     "qlb_transpile_gpu": [_P, _U64, ctypes.POINTER(PoolView), _U32, ctypes.POINTER(TranspileConfig),

@@ -8,6 +8,8 @@ float32, as the reference builder does (frontend.hpp:280-292).
   random_rot_cz      30-qubit depth-24 RX/RY/RZ + random disjoint CZ pairs
   qft                quantum Fourier transform: H + CP(pi/2^j) ladders + swaps
   hea                hardware-efficient ansatz layer (RY, RZ, CZ ladder)
+  hea_batch          the batched workload: HEA circuits with log-uniform
+                     sizes in [10, 20] qubits and depths U{8..32}
   clustered          the reference benchmark's clustered H + CX-chain circuit
                      (benchmarks/bench_hw_awareness.cpp:30-53)
 """
@@ -94,6 +96,24 @@ def hea(n: int, depth: int, seed: int) -> IRModule:
         for i in range(n - 1):
             qc.cz(i, i + 1)
     return qc.release()
+
+
+def hea_batch(count: int = 4096, seed: int = 2024, n_min: int = 10, n_max: int = 20,
+              d_min: int = 8, d_max: int = 32) -> list[IRModule]:
+    """`count` HEA circuits: n = round(exp(U[ln n_min, ln n_max])), depth
+    ~ U{d_min..d_max}, angles from the same seeded stream."""
+    rng = np.random.default_rng(seed)
+    ns = np.rint(np.exp(rng.uniform(math.log(n_min), math.log(n_max), size=count))).astype(int)
+    ds = rng.integers(d_min, d_max + 1, size=count)
+    seeds = rng.integers(0, 2**31 - 1, size=count)
+    return [hea(int(n), int(d), int(sd)) for n, d, sd in zip(ns, ds, seeds)]
+
+
+def expect_z_of(state: np.ndarray, n: int) -> np.ndarray:
+    """<Z_q> = sum |a|^2 (1 - 2 bit_q) of a state vector (FP64)."""
+    p = np.abs(np.asarray(state, dtype=np.complex128)) ** 2
+    idx = np.arange(p.size, dtype=np.int64)
+    return np.array([p.sum() - 2.0 * p[((idx >> q) & 1) == 1].sum() for q in range(n)])
 
 
 def clustered(n: int, cluster: int = 6, depth: int = 15) -> IRModule:

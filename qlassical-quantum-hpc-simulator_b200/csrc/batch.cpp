@@ -1,0 +1,388 @@
+// batch.cpp -- batched execution of many independent circuits (qlb_batch).
+//
+// Every circuit is planned on its own (tile passes, k <= 5 fusion inside
+// tiles, deferred diagonals) by host threads; the plans are merged into one
+// device program.  Round r applies the r-th pass of every circuit that has
+// one, as ONE launch of the tile kernel over a work list of (state, pass)
+// entries, so small circuits share the GPU's 148 SMs instead of each
+// occupying a launch.  |0...0> set-up, all rounds and the FP64 <Z_i>
+// reduction are captured once into a CUDA graph; qlb_batch_run() is one
+// graph launch.  Circuits below 13 qubits run padded to one 13-qubit tile
+// (the extra qubits stay |0>).  With mode -1 the batch is planned both ways
+// (FP32 CUDA-core tiles and tensor-core fused tiles), each graph is timed
+// once, and the faster one is kept.
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <memory>
+#include <thread>
+#include <vector>
+
+#include "abi.h"
+#include "batch.h"
+#include "engine.h"
+#include "kernels.h"
+#include "plan.h"
+#include "tile.h"
+
+using namespace qlb;
+
+namespace {
+
+size_t align256(size_t x) { return (x + 255) & ~size_t{255}; }
+
+struct BatchRound {
+    size_t work_off;     // byte offset of its TileWork entries
+    uint32_t n_work;
+    uint64_t tiles;
+    int has_tc;
+};
+
+// One mode's device program and graph over the shared state buffer.
+struct BatchProgram {
+    int mode = QLB_MODE_TILED;
+    DeviceBuffer dev;                // passes | phases | ops | mats | work lists
+    size_t o_pass = 0, o_phase = 0, o_ops = 0, o_mat = 0;
+    std::vector<BatchRound> rounds;
+    uint64_t tiles = 0, passes = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    float graph_ms = 0.f;
+    ~BatchProgram() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+}  // namespace
+
+struct qlb_batch {
+    cudaStream_t stream = nullptr;
+    uint32_t count = 0;
+    std::vector<BatchState> states;
+    std::vector<uint64_t> chunk_begin;     // count + 1
+    uint64_t total_amps = 0, amp_updates = 0;
+    DeviceBuffer state_buf, meta, partial, result, err;
+    PinnedBuffer host_result, host_err;
+    size_t o_states = 0, o_chunks = 0;
+    std::unique_ptr<BatchProgram> prog;
+    float autotune_ms[2] = {0.f, 0.f};
+    ~qlb_batch() {
+        prog.reset();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+std::unique_ptr<BatchProgram> build_program(qlb_batch& b, int mode, const qlb_gate_instr* const* programs,
+                                            const uint64_t* counts, const qlb_pool_view* pools) {
+    const uint32_t C = b.count;
+    std::vector<HostPlan> plans(C);
+    {
+        std::atomic<uint32_t> next{0};
+        std::vector<std::string> errs(C);
+        std::vector<int> codes(C, 0);
+        auto worker = [&] {
+            for (uint32_t c; (c = next.fetch_add(1)) < C;) {
+                try {
+                    const PlanConfig cfg{b.states[c].eff_qubits, mode, 0, 10.0};
+                    plans[c] = plan_host(cfg, programs[c], counts[c], &pools[c]);
+                } catch (const Error& e) {
+                    codes[c] = e.code;
+                    errs[c] = e.msg;
+                }
+            }
+        };
+        unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        nt = std::min<unsigned>(nt, C);
+        std::vector<std::thread> th;
+        for (unsigned i = 1; i < nt; ++i) th.emplace_back(worker);
+        worker();
+        for (auto& t : th) t.join();
+        for (uint32_t c = 0; c < C; ++c)
+            if (codes[c]) fail(static_cast<qlb_status>(codes[c]), "circuit " + std::to_string(c) + ": " + errs[c]);
+    }
+    // merge
+    auto P = std::make_unique<BatchProgram>();
+    P->mode = mode;
+    TileProgram all;
+    std::vector<std::vector<uint32_t>> pass_ids(C);
+    size_t max_passes = 0;
+    for (uint32_t c = 0; c < C; ++c) {
+        HostPlan& h = plans[c];
+        for (const PlanStep& st : h.steps)
+            if (st.kind != STEP_PASS)
+                fail(QLB_ERR_INVALID_ARG, "circuit " + std::to_string(c) +
+                                              ": batched circuits may hold only gates (no MEASURE, no 6-qubit "
+                                              "blocks, no physical GLOBAL_SWAP)");
+        if (all.mats.size() & 1) all.mats.push_back(make_float2(0.f, 0.f));
+        const uint32_t pb = static_cast<uint32_t>(all.passes.size());
+        const uint32_t phb = static_cast<uint32_t>(all.phases.size());
+        const uint32_t ob = static_cast<uint32_t>(all.ops.size());
+        const uint32_t mb = static_cast<uint32_t>(all.mats.size());
+        for (TilePass p : h.prog.passes) {
+            p.phase_begin += phb;
+            p.phase_end += phb;
+            all.passes.push_back(p);
+        }
+        for (TilePhase ph : h.prog.phases) {
+            ph.op_begin += ob;
+            ph.op_end += ob;
+            all.phases.push_back(ph);
+        }
+        for (TileOp op : h.prog.ops) {
+            op.data += mb;
+            all.ops.push_back(op);
+        }
+        all.mats.insert(all.mats.end(), h.prog.mats.begin(), h.prog.mats.end());
+        for (const PlanStep& st : h.steps) pass_ids[c].push_back(pb + st.index);
+        max_passes = std::max(max_passes, pass_ids[c].size());
+        P->passes += pass_ids[c].size();
+    }
+    // rounds: the r-th pass of every circuit that has one
+    std::vector<TileWork> work;
+    for (size_t r = 0; r < max_passes; ++r) {
+        BatchRound R{work.size() * sizeof(TileWork), 0, 0, 0};
+        for (uint32_t c = 0; c < C; ++c) {
+            if (r >= pass_ids[c].size()) continue;
+            const uint32_t pid = pass_ids[c][r];
+            work.push_back(TileWork{nullptr, R.tiles, nullptr, nullptr, nullptr, nullptr, pid, 0});
+            // state pointers are filled in below, once the buffer exists
+            work.back().pad = c;
+            R.tiles += uint64_t{1} << (b.states[c].eff_qubits - kTileQubits);
+            R.n_work += 1;
+            R.has_tc |= all.passes[pid].has_tc;
+        }
+        P->tiles += R.tiles;
+        P->rounds.push_back(R);
+    }
+    P->o_pass = 0;
+    P->o_phase = align256(all.passes.size() * sizeof(TilePass));
+    P->o_ops = align256(P->o_phase + all.phases.size() * sizeof(TilePhase));
+    P->o_mat = align256(P->o_ops + all.ops.size() * sizeof(TileOp));
+    const size_t o_work = align256(P->o_mat + all.mats.size() * sizeof(float2));
+    const size_t total = align256(o_work + work.size() * sizeof(TileWork));
+    char* d = static_cast<char*>(P->dev.ensure(total));
+    float2* base = static_cast<float2*>(b.state_buf.p);
+    for (TileWork& w : work) {
+        w.state = base + b.states[w.pad].offset;
+        w.pad = 0;
+        w.passes = reinterpret_cast<const TilePass*>(d + P->o_pass);
+        w.phases = reinterpret_cast<const TilePhase*>(d + P->o_phase);
+        w.ops = reinterpret_cast<const TileOp*>(d + P->o_ops);
+        w.mats = reinterpret_cast<const float2*>(d + P->o_mat);
+    }
+    std::vector<char> h(total, 0);
+    std::memcpy(h.data() + P->o_pass, all.passes.data(), all.passes.size() * sizeof(TilePass));
+    std::memcpy(h.data() + P->o_phase, all.phases.data(), all.phases.size() * sizeof(TilePhase));
+    std::memcpy(h.data() + P->o_ops, all.ops.data(), all.ops.size() * sizeof(TileOp));
+    std::memcpy(h.data() + P->o_mat, all.mats.data(), all.mats.size() * sizeof(float2));
+    std::memcpy(h.data() + o_work, work.data(), work.size() * sizeof(TileWork));
+    for (BatchRound& R : P->rounds) R.work_off += o_work;
+    check_cuda(cudaMemcpy(d, h.data(), total, cudaMemcpyHostToDevice), "batch program upload");
+    return P;
+}
+
+void capture(qlb_batch& b, BatchProgram& P) {
+    check_cuda(configure_tile_kernel(), "tile kernel attributes");
+    const char* d = static_cast<const char*>(P.dev.p);
+    const auto* st = reinterpret_cast<const BatchState*>(static_cast<const char*>(b.meta.p) + b.o_states);
+    const auto* chunks = reinterpret_cast<const uint64_t*>(static_cast<const char*>(b.meta.p) + b.o_chunks);
+    float2* base = static_cast<float2*>(b.state_buf.p);
+    int* err = static_cast<int*>(b.err.p);
+    cudaStream_t s = b.stream;
+    check_cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+    cudaError_t e = cudaMemsetAsync(base, 0, b.total_amps * sizeof(float2), s);
+    if (e == cudaSuccess) e = launch_set_basis(base, st, b.count, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), s);
+    for (const BatchRound& R : P.rounds) {
+        if (e != cudaSuccess) break;
+        e = launch_tile_work(reinterpret_cast<const TileWork*>(d + R.work_off), R.n_work, R.tiles, R.has_tc, err, s);
+    }
+    if (e == cudaSuccess)
+        e = launch_batch_expect_z(base, st, b.count, chunks, b.chunk_begin.back(), static_cast<double*>(b.partial.p),
+                                  static_cast<double*>(b.result.p), kBatchStride, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b.host_result.p, b.result.p, static_cast<size_t>(b.count) * kBatchStride * sizeof(double),
+                            cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b.host_err.p, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(s, &g);
+    check_cuda(e, "batch capture");
+    check_cuda(ee, "end capture");
+    P.graph = g;
+    check_cuda(cudaGraphInstantiate(&P.exec, g, 0), "graph instantiate");
+}
+
+float time_graph(qlb_batch& b, BatchProgram& P) {
+    check_cuda(cudaGraphLaunch(P.exec, b.stream), "graph launch");   // warm
+    cudaEvent_t t0, t1;
+    check_cuda(cudaEventCreate(&t0), "event");
+    check_cuda(cudaEventCreate(&t1), "event");
+    cudaEventRecord(t0, b.stream);
+    cudaError_t e = cudaGraphLaunch(P.exec, b.stream);
+    cudaEventRecord(t1, b.stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(t1);
+    float ms = 0.f;
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    check_cuda(e, "autotune run");
+    if (*static_cast<int*>(b.host_err.p) != 0) fail(QLB_ERR_TIMEOUT, "a tile-kernel wait gave up during autotuning");
+    return ms;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qlb_batch_create(qlb_batch_t* out, uint32_t count, const qlb_gate_instr* const* programs, const uint64_t* counts,
+                     const qlb_pool_view* pools, const uint32_t* num_qubits, int mode) {
+    return guarded([&] {
+        need(out, "out");
+        *out = nullptr;
+        if (count == 0) fail(QLB_ERR_INVALID_ARG, "empty batch");
+        need(programs, "programs");
+        need(counts, "counts");
+        need(pools, "pools");
+        need(num_qubits, "num_qubits");
+        if (mode != QLB_MODE_TILED && mode != QLB_MODE_TILED_TC && mode != -1)
+            fail(QLB_ERR_INVALID_ARG, "batch mode must be QLB_MODE_TILED, QLB_MODE_TILED_TC or -1 (autotune)");
+        auto b = std::make_unique<qlb_batch>();
+        b->count = count;
+        b->states.resize(count);
+        b->chunk_begin.resize(count + 1);
+        uint64_t off = 0, chunks = 0;
+        for (uint32_t c = 0; c < count; ++c) {
+            const uint32_t n = num_qubits[c];
+            if (n == 0 || n > 30) fail(QLB_ERR_INVALID_ARG, "batched circuits take 1..30 qubits");
+            if (counts[c] && !programs[c]) fail(QLB_ERR_INVALID_ARG, "null program");
+            const uint32_t ne = std::max(n, kBatchMinQubits);
+            b->states[c] = BatchState{off, n, ne};
+            b->chunk_begin[c] = chunks;
+            off += uint64_t{1} << ne;
+            chunks += uint64_t{1} << (ne - kBatchMinQubits);
+            for (uint64_t i = 0; i < counts[c]; ++i) {
+                const qlb_gate_instr& g = programs[c][i];
+                if (g.type != QLB_BARRIER && g.type != QLB_MEASURE)
+                    b->amp_updates += uint64_t{1} << n;
+            }
+        }
+        b->chunk_begin[count] = chunks;
+        b->total_amps = off;
+        check_cuda(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "stream");
+        b->state_buf.ensure(off * sizeof(float2));
+        b->o_states = 0;
+        b->o_chunks = align256(count * sizeof(BatchState));
+        const size_t meta_bytes = b->o_chunks + (count + 1) * sizeof(uint64_t);
+        char* m = static_cast<char*>(b->meta.ensure(meta_bytes));
+        check_cuda(cudaMemcpy(m + b->o_states, b->states.data(), count * sizeof(BatchState), cudaMemcpyHostToDevice),
+                   "batch states");
+        check_cuda(cudaMemcpy(m + b->o_chunks, b->chunk_begin.data(), (count + 1) * sizeof(uint64_t),
+                              cudaMemcpyHostToDevice),
+                   "batch chunks");
+        b->partial.ensure(batch_partial_doubles(chunks) * sizeof(double));
+        b->result.ensure(static_cast<size_t>(count) * kBatchStride * sizeof(double));
+        b->err.ensure(256);
+        b->host_result.ensure(static_cast<size_t>(count) * kBatchStride * sizeof(double));
+        b->host_err.ensure(sizeof(int));
+        *static_cast<int*>(b->host_err.p) = 0;
+        if (mode == -1) {
+            auto p0 = build_program(*b, QLB_MODE_TILED, programs, counts, pools);
+            capture(*b, *p0);
+            b->autotune_ms[0] = time_graph(*b, *p0);
+            auto p1 = build_program(*b, QLB_MODE_TILED_TC, programs, counts, pools);
+            capture(*b, *p1);
+            b->autotune_ms[1] = time_graph(*b, *p1);
+            b->prog = b->autotune_ms[1] < b->autotune_ms[0] ? std::move(p1) : std::move(p0);
+        } else {
+            b->prog = build_program(*b, mode, programs, counts, pools);
+            capture(*b, *b->prog);
+        }
+        *out = b.release();
+    });
+}
+
+int qlb_batch_run(qlb_batch_t b) {
+    return guarded([&] {
+        need(b, "batch");
+        check_cuda(cudaGraphLaunch(b->prog->exec, b->stream), "batch graph launch");
+    });
+}
+
+int qlb_batch_synchronize(qlb_batch_t b) {
+    return guarded([&] {
+        need(b, "batch");
+        check_cuda(cudaStreamSynchronize(b->stream), "batch sync");
+        if (*static_cast<int*>(b->host_err.p) != 0)
+            fail(QLB_ERR_TIMEOUT, "a tile-kernel wait gave up (copy or tensor-core completion)");
+    });
+}
+
+int qlb_batch_expect_z(qlb_batch_t b, double* out, uint32_t stride) {
+    return guarded([&] {
+        need(b, "batch");
+        need(out, "out");
+        const double* r = static_cast<const double*>(b->host_result.p);
+        for (uint32_t c = 0; c < b->count; ++c) {
+            if (stride < b->states[c].num_qubits) fail(QLB_ERR_INVALID_ARG, "stride below a circuit's qubit count");
+            for (uint32_t q = 0; q < b->states[c].num_qubits; ++q)
+                out[static_cast<uint64_t>(c) * stride + q] = r[static_cast<uint64_t>(c) * kBatchStride + q];
+        }
+    });
+}
+
+int qlb_batch_state(qlb_batch_t b, uint32_t index, double* out_c128, uint64_t dim) {
+    return guarded([&] {
+        need(b, "batch");
+        need(out_c128, "out");
+        if (index >= b->count) fail(QLB_ERR_INVALID_ARG, "circuit index out of range");
+        const BatchState& s = b->states[index];
+        if (dim != (uint64_t{1} << s.num_qubits)) fail(QLB_ERR_INVALID_ARG, "dim must be 2^num_qubits");
+        check_cuda(cudaStreamSynchronize(b->stream), "batch sync");
+        std::vector<float2> h(dim);
+        check_cuda(cudaMemcpy(h.data(), static_cast<float2*>(b->state_buf.p) + s.offset, dim * sizeof(float2),
+                              cudaMemcpyDeviceToHost),
+                   "batch state D2H");
+        for (uint64_t i = 0; i < dim; ++i) {
+            out_c128[2 * i] = h[i].x;
+            out_c128[2 * i + 1] = h[i].y;
+        }
+    });
+}
+
+int qlb_batch_stats(qlb_batch_t b, qlb_batch_info* out) {
+    return guarded([&] {
+        need(b, "batch");
+        need(out, "out");
+        out->circuits = b->count;
+        out->rounds = static_cast<uint32_t>(b->prog->rounds.size());
+        out->mode = b->prog->mode;
+        out->launches = static_cast<uint32_t>(b->prog->rounds.size()) + 4;
+        out->tiles = b->prog->tiles;
+        out->passes = b->prog->passes;
+        out->amp_updates = b->amp_updates;
+        out->state_bytes = b->total_amps * sizeof(float2);
+        out->autotune_ms[0] = b->autotune_ms[0];
+        out->autotune_ms[1] = b->autotune_ms[1];
+    });
+}
+
+int qlb_batch_stream(qlb_batch_t b, void** out) {
+    return guarded([&] {
+        need(b, "batch");
+        need(out, "out");
+        *out = b->stream;
+    });
+}
+
+int qlb_batch_destroy(qlb_batch_t b) {
+    return guarded([&] {
+        if (!b) return;
+        cudaStreamSynchronize(b->stream);
+        delete b;
+    });
+}
+
+}  // extern "C"

@@ -14,6 +14,7 @@
 // the same result as physically swapping and un-permuting at read-out.
 // With the physical option it moves the data (a swap kernel, one
 // bandwidth-bound pass) and restores logical order when execute() returns.
+#include "abi.h"
 #include "engine.h"
 
 #include <algorithm>
@@ -300,30 +301,6 @@ void apply_plain(qlb_engine& e, const qlb_gate_instr& in, const float2* mat) {
 using namespace qlb;
 
 namespace {
-
-template <typename F>
-int guarded(F&& f) {
-    try {
-        f();
-        return QLB_OK;
-    } catch (const Error& err) {
-        g_last_error = err.msg;
-        return err.code;
-    } catch (const std::bad_alloc&) {
-        g_last_error = "host allocation failed";
-        return QLB_ERR_OOM;
-    } catch (const std::exception& ex) {
-        g_last_error = ex.what();
-        return QLB_ERR_CUDA;
-    } catch (...) {
-        g_last_error = "unknown error";
-        return QLB_ERR_CUDA;
-    }
-}
-
-void need(const void* p, const char* what) {
-    if (!p) fail(QLB_ERR_INVALID_ARG, std::string(what) + " is null");
-}
 
 uint32_t log2_exact(uint64_t dim) {
     if (dim == 0 || (dim & (dim - 1)) != 0)
@@ -643,7 +620,7 @@ int qlb_describe_plan(uint32_t n, int mode, int physical, const qlb_gate_instr* 
         if (n > 34) fail(QLB_ERR_INVALID_ARG, "at most 34 qubits");
         if (mode < QLB_MODE_PLAIN || mode > QLB_MODE_TILED_TC) fail(QLB_ERR_INVALID_ARG, "unknown execution mode");
         for (uint64_t i = 0; i < count; ++i) validate_instr(prog[i], n, pool);
-        const std::string js = describe_plan_json(PlanConfig{n, mode, physical}, prog, count, pool);
+        const std::string js = describe_plan_json(PlanConfig{n, mode, physical, 10.0}, prog, count, pool);
         if (needed) *needed = js.size() + 1;
         if (out && cap) {
             const size_t m = std::min<size_t>(cap - 1, js.size());
@@ -684,8 +661,14 @@ int qlb_engine_set_mode(qlb_engine_t e, int mode) {
 int qlb_engine_set_option(qlb_engine_t e, int key, int64_t value) {
     return guarded([&] {
         need(e, "engine");
-        if (key == QLB_OPT_PHYSICAL_GLOBAL_SWAP) e->physical_global_swap = value != 0;
-        else fail(QLB_ERR_INVALID_ARG, "unknown engine option");
+        if (key == QLB_OPT_PHYSICAL_GLOBAL_SWAP) {
+            e->physical_global_swap = value != 0;
+        } else if (key == QLB_OPT_TC_MIN_COST) {
+            if (value < 0) fail(QLB_ERR_INVALID_ARG, "QLB_OPT_TC_MIN_COST must be >= 0");
+            e->tc_min_cost = static_cast<double>(value) / 100.0;
+        } else {
+            fail(QLB_ERR_INVALID_ARG, "unknown engine option");
+        }
     });
 }
 int qlb_engine_get_mode(qlb_engine_t e, int* mode) {

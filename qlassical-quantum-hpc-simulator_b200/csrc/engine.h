@@ -63,6 +63,7 @@ struct qlb_engine {
     std::vector<uint8_t> measurements;
     int mode = QLB_MODE_TILED;
     int physical_global_swap = 0;   // execute GLOBAL_SWAP as a data permutation
+    double tc_min_cost = 10.0;      // TILED_TC: smallest fused-run cost sent to the tensor cores
     qlb::DeviceBuffer red_partial, red_out, staging, err_flag;   // err_flag: device int set by bounded waits
     qlb::PinnedBuffer host_pinned, host_prog;
     qlb_exec_stats stats{};

@@ -43,10 +43,18 @@ struct PlanConfig {
     uint32_t n;
     int mode;
     int physical_global_swap;
+    double tc_min_cost = 10.0;   // TILED_TC: smallest fused-run cost sent to the tensor cores
 };
 // Host-only planning: the plan as JSON (steps, passes, phases, ops, matrices).
 std::string describe_plan_json(const PlanConfig& cfg, const qlb_gate_instr* prog, uint64_t count,
                                const qlb_pool_view* pool);
+// Host-only planning result (no device memory touched).
+struct HostPlan {
+    std::vector<PlanStep> steps;
+    TileProgram prog;
+    qlb_exec_stats stats{};
+};
+HostPlan plan_host(const PlanConfig& cfg, const qlb_gate_instr* prog, uint64_t count, const qlb_pool_view* pool);
 // Builds a plan for the engine's qubit count, mode and options.
 qlb_plan* compile_plan(qlb_engine& e, const qlb_gate_instr* prog, uint64_t count, const qlb_pool_view* pool);
 void run_plan(qlb_engine& e, const qlb_plan& p);

@@ -147,6 +147,7 @@ struct PhaseBuild {
     std::vector<int> reg;            // tile-local positions, register bit order
     std::vector<uint32_t> ops;       // indices into the mapped stream
     int dense_k = 0;                 // 0 or the k of the DENSE op placed at bits 0..k-1
+    uint64_t thr_mem[kThreadQubits] = {};   // memory qubit of thread bit j (set before encoding)
 };
 
 void choose_threads(const std::vector<int>& reg, bool edge, uint8_t* thr) {
@@ -267,7 +268,9 @@ public:
                 T = nt;
                 taken.push_back(idx);
             }
-            build_pass(T, taken);
+            // deferred diagonal terms may ride into the next pass unless a
+            // plain step (measurement, data permutation) or the end follows
+            build_pass(T, taken, rest.empty() || mi[rest.front()].plain);
             pending.swap(rest);
         }
         if (permuted) {
@@ -326,7 +329,7 @@ private:
     const qlb_pool_view* pool_;
     uint32_t n_;
 
-    void build_pass(uint64_t T, const std::vector<uint32_t>& ops) {
+    void build_pass(uint64_t T, const std::vector<uint32_t>& ops, bool final_pass) {
         // fill the tile with the lowest unused memory qubits
         for (uint32_t q = 0; q < n_ && __builtin_popcountll(T) < kTileQubits; ++q) T |= bitm(q);
         TilePass P{};
@@ -412,19 +415,20 @@ private:
             TilePhase ph{};
             for (int r = 0; r < kRegQubits; ++r) ph.reg_pos[r] = static_cast<uint8_t>(pb.reg[r]);
             choose_threads(pb.reg, edge, ph.thr_pos);
+            for (int j = 0; j < kThreadQubits; ++j) pb.thr_mem[j] = bitm(P.tile_pos[ph.thr_pos[j]]);
             ph.op_begin = static_cast<uint32_t>(prog.ops.size());
-            encode_ops(pb, P, local_of, pi + 1 == phases.size());
+            encode_ops(pb, P, local_of, final_pass && pi + 1 == phases.size());
             ph.op_end = static_cast<uint32_t>(prog.ops.size());
             prog.phases.push_back(ph);
         }
         P.phase_end = static_cast<uint32_t>(prog.phases.size());
         P.n_low = 0;
         while (P.n_low < kTileQubits && P.tile_pos[P.n_low] == P.n_low) ++P.n_low;
-        P.has_tc = pass_has_tc_ ? 1 : 0;
+        P.has_tc = static_cast<uint8_t>(pass_features_);
         PlanStep st{};
         st.kind = STEP_PASS;
         st.has_tc = P.has_tc;
-        pass_has_tc_ = false;
+        pass_features_ = 0;
         st.index = static_cast<uint32_t>(prog.passes.size());
         steps.push_back(st);
         prog.passes.push_back(P);
@@ -454,7 +458,7 @@ private:
     // Accumulated global phase of the pass being built (constant terms of
     // RZ and diagonal UNITARYs); applied once at the end of its last phase.
     double pass_global_ = 0.0;
-    bool pass_has_tc_ = false;
+    int pass_features_ = 0;   // kPass* bits of the pass being built
 
     // ---- FP64 form of one register-level op --------------------------------
     using cd = std::complex<double>;
@@ -634,6 +638,7 @@ private:
             break;
         case TOP_SWAP:
             op.code = static_cast<uint16_t>(OPC_SWAP + reg_pair_index(r0, static_cast<uint32_t>(h.r1)));
+            pass_features_ |= kPassWide;
             break;
         case TOP_CPHASE:
             op.code = OPC_CPHASE;
@@ -649,6 +654,7 @@ private:
             for (const cd& z : h.mat) prog.mats.push_back(f2(z));
             if (prog.mats.size() & 1) prog.mats.push_back(make_float2(0.f, 0.f));
             if (h.kind == TOP_DENSE) stats.dense_ops += 1;
+            pass_features_ |= kPassWide;
             break;
         }
         default: break;
@@ -698,7 +704,7 @@ private:
         prog.ops.push_back(op);
         stats.dense_ops += 1;
         stats.tc_ops += 1;
-        pass_has_tc_ = true;
+        pass_features_ |= kPassTensorCores | kPassWide;
     }
 
     // Register-local ops waiting to be fused into one tensor-core op.
@@ -710,7 +716,7 @@ private:
 
     void flush(Acc& acc) {
         if (acc.ops.empty()) return;
-        if (acc.cost < 10.0) {     // cheaper as individual CUDA-core ops
+        if (acc.cost < e_.tc_min_cost) {     // cheaper as individual CUDA-core ops
             for (const HostOp& h : acc.ops) emit_cuda_op(h);
         } else {
             std::vector<cd> U(32 * 32, cd(0.0, 0.0));
@@ -804,6 +810,8 @@ private:
         bool has_r = false;
         std::vector<PTerm> T;                                   // thread / memory-bit terms
         std::vector<std::pair<uint64_t, uint32_t>> S;           // mixed pi terms
+        uint64_t thr_mask = 0;                                  // memory qubits on thread bits
+        for (int j = 0; j < kThreadQubits; ++j) thr_mask |= pb.thr_mem[j];
         struct G {
             uint64_t cmem;
             uint32_t cm;
@@ -877,7 +885,41 @@ private:
         T.erase(std::remove_if(T.begin(), T.end(), [](const PTerm& t) { return is_one(t.p1) && is_one(t.p0); }),
                 T.end());
         S.erase(std::remove_if(S.begin(), S.end(), [](const auto& x) { return x.second == 0u; }), S.end());
-        if (!has_r && T.empty() && S.empty() && Gs.empty()) return;
+        // Terms on thread bits only become per-thread tables (one load per
+        // thread); terms touching out-of-tile qubits stay as lists.
+        auto thread_bits = [&](uint32_t t) {
+            uint64_t m = 0;
+            for (int j = 0; j < kThreadQubits; ++j)
+                if ((t >> j) & 1u) m |= pb.thr_mem[j];
+            return m;
+        };
+        std::vector<cd> ttab;
+        std::vector<uint32_t> stab;
+        {
+            std::vector<PTerm> keep;
+            for (const PTerm& t : T) {
+                if (t.mask != 0 && (t.mask & ~thr_mask) == 0) {
+                    if (ttab.empty()) ttab.assign(256, cd(1.0, 0.0));
+                    for (uint32_t th = 0; th < 256; ++th)
+                        ttab[th] *= ((thread_bits(th) & t.mask) == t.mask) ? t.p1 : t.p0;
+                } else {
+                    keep.push_back(t);
+                }
+            }
+            T.swap(keep);
+            std::vector<std::pair<uint64_t, uint32_t>> skeep;
+            for (const auto& x : S) {
+                if ((x.first & ~thr_mask) == 0) {
+                    if (stab.empty()) stab.assign(256, 0u);
+                    for (uint32_t th = 0; th < 256; ++th)
+                        if ((thread_bits(th) & x.first) == x.first) stab[th] ^= x.second;
+                } else {
+                    skeep.push_back(x);
+                }
+            }
+            S.swap(skeep);
+        }
+        if (!has_r && ttab.empty() && stab.empty() && T.empty() && S.empty() && Gs.empty()) return;
         if (T.size() > 0xFFFF || S.size() > 0xFFFF) fail(QLB_ERR_INVALID_ARG, "too many diagonal terms in one pass");
         auto f2 = [](cd z) { return make_float2(static_cast<float>(z.real()), static_cast<float>(z.imag())); };
         auto words = [&](uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
@@ -897,11 +939,18 @@ private:
         op.kind = TOP_DIAG;
         op.code = OPC_DIAG;
         op.data = static_cast<uint32_t>(prog.mats.size());
-        op.flags = has_r ? 1u : 0u;
+        op.flags = (has_r ? 1u : 0u) | (ttab.empty() ? 0u : 2u) | (stab.empty() ? 0u : 4u);
         op.n = static_cast<uint32_t>(T.size()) | (static_cast<uint32_t>(S.size()) << 16);
         op.ctrl_reg = static_cast<uint32_t>(Gs.size());
         if (has_r)
             for (uint32_t m = 0; m < 32; ++m) prog.mats.push_back(f2(R[m]));
+        for (const cd& z : ttab) prog.mats.push_back(f2(z));
+        for (size_t th = 0; th < stab.size(); th += 2) {
+            float2 f;
+            std::memcpy(&f.x, &stab[th], 4);
+            std::memcpy(&f.y, &stab[th + 1], 4);
+            prog.mats.push_back(f);
+        }
         for (const PTerm& t : T) {
             const float2 a = f2(t.p1), b = f2(t.p0);
             words(static_cast<uint32_t>(t.mask), static_cast<uint32_t>(t.mask >> 32), bits(a.x), bits(a.y));
@@ -977,8 +1026,19 @@ size_t align256(size_t x) { return (x + 255) & ~size_t{255}; }
 
 }  // namespace
 
+HostPlan plan_host(const PlanConfig& cfg, const qlb_gate_instr* prog, uint64_t count, const qlb_pool_view* pool) {
+    Planner pl(cfg, pool);
+    pl.plan(prog, count);
+    HostPlan h;
+    h.steps = std::move(pl.steps);
+    h.prog = std::move(pl.prog);
+    h.stats = pl.stats;
+    h.stats.instructions = count;
+    return h;
+}
+
 qlb_plan* compile_plan(qlb_engine& e, const qlb_gate_instr* prog, uint64_t count, const qlb_pool_view* pool) {
-    Planner pl(PlanConfig{e.sv.n, e.mode, e.physical_global_swap}, pool);
+    Planner pl(PlanConfig{e.sv.n, e.mode, e.physical_global_swap, e.tc_min_cost}, pool);
     pl.plan(prog, count);
     TileProgram& tp = pl.prog;
     auto* p = new qlb_plan();

@@ -409,10 +409,21 @@ __device__ __forceinline__ bool op_dense_tc(float2 (&v)[NR], const float2* __res
 
 // TOP_DIAG: the per-thread factor of the thread/memory-bit terms, the sign
 // mask of the mixed pi terms, then one complex multiply per amplitude.
-__device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* __restrict__ tab, uint32_t has_r,
+__device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* __restrict__ tab, uint32_t flags,
                                         uint32_t n_t, uint32_t n_s, uint32_t n_g, uint64_t gt) {
-    const uint4* p = reinterpret_cast<const uint4*>(tab) + (has_r ? 16 : 0);
+    const uint32_t has_r = flags & 1u;
+    const float2* q = tab + (has_r ? 32 : 0);
     float2 T = make_float2(1.f, 0.f);
+    if (flags & 2u) {
+        T = __ldg(q + threadIdx.x);
+        q += 256;
+    }
+    uint32_t smask = 0;
+    if (flags & 4u) {
+        smask = __ldg(reinterpret_cast<const uint32_t*>(q) + threadIdx.x);
+        q += 128;
+    }
+    const uint4* p = reinterpret_cast<const uint4*>(q);
 #pragma unroll 2
     for (uint32_t t = 0; t < n_t; ++t) {
         const uint4 w0 = __ldg(p + 2 * t), w1 = __ldg(p + 2 * t + 1);
@@ -423,7 +434,6 @@ __device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* __restric
         T = cmul(T, f);
     }
     p += 2 * n_t;
-    uint32_t smask = 0;
 #pragma unroll 4
     for (uint32_t t = 0; t < n_s; ++t) {
         const uint4 w = __ldg(p + t);
@@ -460,8 +470,15 @@ __device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* __restric
 
 __device__ __forceinline__ float2 f2(uint32_t a, uint32_t b) { return make_float2(__uint_as_float(a), __uint_as_float(b)); }
 
+__device__ __forceinline__ void op_cphase(float2 (&v)[NR], uint32_t cm, float2 p) {
+#pragma unroll
+    for (int i = 0; i < NR; ++i)
+        if ((static_cast<uint32_t>(i) & cm) == cm) v[i] = cmul(v[i], p);
+}
+
 // The op loop of one phase.  Each op is four 16-byte words; the first holds
 // the dispatch code, the register controls and the data offset.
+template <bool WIDE>
 __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, const TileOp* ops,
                                         const float2* __restrict__ mats, float2* sm, const PhaseMap& M,
                                         bool linear, TcCtx& tc) {
@@ -474,7 +491,6 @@ __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, co
             if ((M.gt & c) != c) continue;
         }
         const uint32_t cm = q0.z, data = q0.w;
-        switch (q0.x & 0xFFFFu) {
 #define QLB_U1R_CASE(RR)                                                                              \
     case OPC_U1R + RR: {                                                                              \
         const uint4 a = rec[4 * oi + 2], b = rec[4 * oi + 3];                                         \
@@ -508,42 +524,48 @@ __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, co
 #define QLB_PAIR_CASES(A, B)                                                                          \
     case OPC_SWAP + reg_pair_index(A, B): op_swap<A, B>(v, cm); break;                                \
     case OPC_U2 + reg_pair_index(A, B): op_u2<A, B>(v, mats + data, cm); break;
-            QLB_U1R_CASE(0) QLB_U1R_CASE(1) QLB_U1R_CASE(2) QLB_U1R_CASE(3) QLB_U1R_CASE(4)
-            QLB_RX_CASE(0) QLB_RX_CASE(1) QLB_RX_CASE(2) QLB_RX_CASE(3) QLB_RX_CASE(4)
-            QLB_U1_CASE(0) QLB_U1_CASE(1) QLB_U1_CASE(2) QLB_U1_CASE(3) QLB_U1_CASE(4)
-            QLB_X_CASE(0) QLB_X_CASE(1) QLB_X_CASE(2) QLB_X_CASE(3) QLB_X_CASE(4)
-            QLB_PAIR_CASES(0, 1) QLB_PAIR_CASES(0, 2) QLB_PAIR_CASES(0, 3) QLB_PAIR_CASES(0, 4)
-            QLB_PAIR_CASES(1, 2) QLB_PAIR_CASES(1, 3) QLB_PAIR_CASES(1, 4)
-            QLB_PAIR_CASES(2, 3) QLB_PAIR_CASES(2, 4) QLB_PAIR_CASES(3, 4)
+#define QLB_COMMON_CASES                                                                              \
+    QLB_U1R_CASE(0) QLB_U1R_CASE(1) QLB_U1R_CASE(2) QLB_U1R_CASE(3) QLB_U1R_CASE(4)                   \
+    QLB_RX_CASE(0) QLB_RX_CASE(1) QLB_RX_CASE(2) QLB_RX_CASE(3) QLB_RX_CASE(4)                        \
+    QLB_U1_CASE(0) QLB_U1_CASE(1) QLB_U1_CASE(2) QLB_U1_CASE(3) QLB_U1_CASE(4)                        \
+    QLB_X_CASE(0) QLB_X_CASE(1) QLB_X_CASE(2) QLB_X_CASE(3) QLB_X_CASE(4)                             \
+    case OPC_DIAG:                                                                                    \
+        op_diag(v, mats + data, rec[4 * oi + 1].x, rec[4 * oi + 1].y & 0xFFFFu, rec[4 * oi + 1].y >> 16, cm, M.gt); \
+        break;                                                                                        \
+    case OPC_CPHASE:                                                                                  \
+        op_cphase(v, cm, f2(rec[4 * oi + 2].x, rec[4 * oi + 2].y));                                  \
+        break;
+        // Multi-qubit ops live only in the WIDE instantiation, so passes of
+        // 1-qubit and diagonal ops run a kernel with a small code body.
+        if constexpr (WIDE) {
+            switch (q0.x & 0xFFFFu) {
+                QLB_COMMON_CASES
+                QLB_PAIR_CASES(0, 1) QLB_PAIR_CASES(0, 2) QLB_PAIR_CASES(0, 3) QLB_PAIR_CASES(0, 4)
+                QLB_PAIR_CASES(1, 2) QLB_PAIR_CASES(1, 3) QLB_PAIR_CASES(1, 4)
+                QLB_PAIR_CASES(2, 3) QLB_PAIR_CASES(2, 4) QLB_PAIR_CASES(3, 4)
+            case OPC_DENSE3: op_dense_reg<3>(v, mats + data); break;
+            case OPC_DENSE4: op_dense_reg<4>(v, mats + data); break;
+            case OPC_DENSE5: op_dense5(v, mats + data, sm, M, linear); break;
+            case OPC_DENSE_TC:                 // CTA-wide; never controlled
+                if (!op_dense_tc(v, mats + data, sm, tc)) return false;
+                break;
+            default: break;
+            }
+        } else {
+            switch (q0.x & 0xFFFFu) {
+                QLB_COMMON_CASES
+            default: break;
+            }
+        }
+    }
+    return true;
+}
+#undef QLB_COMMON_CASES
 #undef QLB_U1R_CASE
 #undef QLB_RX_CASE
 #undef QLB_U1_CASE
 #undef QLB_X_CASE
 #undef QLB_PAIR_CASES
-        case OPC_DENSE3: op_dense_reg<3>(v, mats + data); break;
-        case OPC_DENSE4: op_dense_reg<4>(v, mats + data); break;
-        case OPC_DENSE5: op_dense5(v, mats + data, sm, M, linear); break;
-        case OPC_DENSE_TC:                 // CTA-wide; never controlled
-            if (!op_dense_tc(v, mats + data, sm, tc)) return false;
-            break;
-        case OPC_DIAG: {
-            const uint4 q1 = rec[4 * oi + 1];
-            op_diag(v, mats + data, q1.x & 1u, q1.y & 0xFFFFu, q1.y >> 16, cm, M.gt);
-            break;
-        }
-        case OPC_CPHASE: {
-            const uint4 a = rec[4 * oi + 2];
-            const float2 p = f2(a.x, a.y);
-#pragma unroll
-            for (int i = 0; i < NR; ++i)
-                if ((static_cast<uint32_t>(i) & cm) == cm) v[i] = cmul(v[i], p);
-            break;
-        }
-        default: break;
-        }
-    }
-    return true;
-}
 
 // Largest i with work[i].tile_begin <= tile (entries sorted by tile_begin).
 __device__ __forceinline__ uint32_t find_work(const TileWork* __restrict__ work, uint32_t n_work, uint64_t tile) {
@@ -561,10 +583,11 @@ __device__ __forceinline__ uint32_t find_work(const TileWork* __restrict__ work,
 // state: one entry passed by value, n_work = 0).  A CTA restages the pass
 // descriptor, phases and ops in shared memory when its next tile belongs to
 // a different pass.
+template <bool WIDE>
 __global__ void __launch_bounds__(NT, 1)
-k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work, uint64_t ntiles,
-            const TilePass* __restrict__ passes, const TilePhase* __restrict__ gphases,
-            const TileOp* __restrict__ gops, const float2* __restrict__ mats, int has_tc, int* __restrict__ err) {
+k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work, uint64_t ntiles, int features,
+            int* __restrict__ err) {
+    const int has_tc = features & kPassTensorCores;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     float2* bufs = reinterpret_cast<float2*>(smem_raw);
     TileOp* sops = reinterpret_cast<TileOp*>(smem_raw + kSmemBuffers);
@@ -594,13 +617,17 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
 
     auto entry = [&](uint64_t t) -> TileWork { return n_work ? work[find_work(work, n_work, t)] : single; };
 
-    // Stage pass `pi`: its descriptor, phases and (if they fit) ops.  Phase
-    // op ranges index the global op array; the shared copy is rebased.
+    // Stage the entry's pass: its descriptor, phases and (if they fit) ops.
+    // Phase op ranges index the program's op array; the shared copy is rebased.
     uint32_t staged = ~0u, nph = 0;
+    const TilePass* staged_prog = nullptr;
     const TilePhase* phases = nullptr;
     const TileOp* ops = nullptr;
-    auto stage = [&](uint32_t pi) {
-        const TilePass& GP = passes[pi];
+    const float2* mats = nullptr;
+    auto stage = [&](const TileWork& w) {
+        const TilePhase* gphases = w.phases;
+        const TileOp* gops = w.ops;
+        const TilePass& GP = w.passes[w.pass];
         {
             const uint32_t* src = reinterpret_cast<const uint32_t*>(&GP);
             uint32_t* dst = reinterpret_cast<uint32_t*>(spass);
@@ -619,21 +646,23 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
                 reinterpret_cast<uint4*>(sops)[i] = reinterpret_cast<const uint4*>(gops + ob)[i];
         phases = ph_in_smem ? sph : gphases + pb;
         ops = ops_in_smem ? sops - ob : gops;
-        staged = pi;
+        mats = w.mats;
+        staged = w.pass;
+        staged_prog = w.passes;
     };
 
     uint64_t tile = blockIdx.x;
     float2* xbuf = bufs + 2 * static_cast<size_t>(TILE);
     if (tile < ntiles) {
         const TileWork w = entry(tile);
-        issue_tile_load(bufs, w.state, passes[w.pass], tile - w.tile_begin, &bar[0]);
+        issue_tile_load(bufs, w.state, w.passes[w.pass], tile - w.tile_begin, &bar[0]);
     }
     uint32_t it = 0;
     for (; tile < ntiles; tile += gridDim.x, ++it) {
         const TileWork w = entry(tile);
-        if (w.pass != staged) {          // uniform: every thread reads the same entry
+        if (w.pass != staged || w.passes != staged_prog) {   // uniform: every thread reads the same entry
             __syncthreads();
-            stage(w.pass);
+            stage(w);
             __syncthreads();
         }
         const TilePass& P = *spass;
@@ -644,7 +673,7 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
         if (next < ntiles) {
             const TileWork wn = entry(next);
             fence_proxy_async();   // earlier generic-proxy reads of nxt precede the async-proxy writes
-            issue_tile_load(nxt, wn.state, passes[wn.pass], next - wn.tile_begin, &bar[b ^ 1u]);
+            issue_tile_load(nxt, wn.state, wn.passes[wn.pass], next - wn.tile_begin, &bar[b ^ 1u]);
         }
         const bool ok = mbar_wait_bounded(&bar[b], (it >> 1) & 1u);
         if (__syncthreads_or(!ok)) {
@@ -659,7 +688,7 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
         PhaseMap M = make_map(P, phases[0], base);
 #pragma unroll
         for (int m = 0; m < NR; ++m) v[m] = cur[local_of(M, m)];
-        bool good = run_ops(v, phases[0], ops, mats, cur, M, true, tc);
+        bool good = run_ops<WIDE>(v, phases[0], ops, mats, cur, M, true, tc);
         // Transposes alternate between the transpose buffer and `cur`: the
         // buffer written at transition k was last read at transition k-2,
         // before barrier k-1, so one barrier per transition suffices.
@@ -673,7 +702,7 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
 #pragma unroll
             for (int m = 0; m < NR; ++m) v[m] = wbuf[slot_of(M, m)];
             rbuf = wbuf;
-            good = run_ops(v, phases[p], ops, mats, rbuf, M, false, tc);
+            good = run_ops<WIDE>(v, phases[p], ops, mats, rbuf, M, false, tc);
         }
         if (!good) {     // a tensor-core wait gave up (every thread agrees)
             if (threadIdx.x == 0) atomicExch(err, 2);
@@ -707,44 +736,53 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
 
 }  // namespace
 
-namespace {
 cudaError_t configure_tile_kernel() {
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_tile_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(k_tile_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              static_cast<int>(kSmemTotal));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_tile_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(kSmemTotal));
         if (e != cudaSuccess) return e;
         configured = true;
     }
     return cudaSuccess;
 }
+
+namespace {
+void launch_tile_kernel(unsigned grid, const TileWork& single, const TileWork* work, uint32_t n_work, uint64_t ntiles,
+                        int features, int* err, cudaStream_t s) {
+    if (features & (kPassWide | kPassTensorCores))
+        k_tile_pass<true><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
+    else
+        k_tile_pass<false><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
+}
 }  // namespace
 
 cudaError_t launch_tile_pass(float2* state, uint32_t n, const TilePass* d_passes, const TilePhase* d_phases,
-                             const TileOp* d_ops, const float2* d_mats, uint32_t pass_index, int has_tc,
+                             const TileOp* d_ops, const float2* d_mats, uint32_t pass_index, int features,
                              int* err, cudaStream_t s) {
     cudaError_t e = configure_tile_kernel();
     if (e != cudaSuccess) return e;
     const uint64_t tiles = uint64_t{1} << (n - kTileQubits);
     uint64_t grid = static_cast<uint64_t>(sm_count());
     if (grid > tiles) grid = tiles;
-    const TileWork single{state, 0, pass_index, 0};
-    k_tile_pass<<<static_cast<unsigned>(grid), NT, kSmemTotal, s>>>(single, nullptr, 0, tiles, d_passes, d_phases,
-                                                                     d_ops, d_mats, has_tc, err);
+    const TileWork single{state, 0, d_passes, d_phases, d_ops, d_mats, pass_index, 0};
+    launch_tile_kernel(static_cast<unsigned>(grid), single, nullptr, 0, tiles, features, err, s);
     return cudaGetLastError();
 }
 
-cudaError_t launch_tile_work(const TileWork* d_work, uint32_t n_work, uint64_t total_tiles, const TilePass* d_passes,
-                             const TilePhase* d_phases, const TileOp* d_ops, const float2* d_mats, int has_tc,
-                             int* err, cudaStream_t s) {
+cudaError_t launch_tile_work(const TileWork* d_work, uint32_t n_work, uint64_t total_tiles, int features, int* err,
+                             cudaStream_t s, uint32_t max_ctas) {
     if (n_work == 0 || total_tiles == 0) return cudaSuccess;
     cudaError_t e = configure_tile_kernel();
     if (e != cudaSuccess) return e;
     uint64_t grid = static_cast<uint64_t>(sm_count());
+    if (max_ctas && grid > max_ctas) grid = max_ctas;
     if (grid > total_tiles) grid = total_tiles;
-    const TileWork none{nullptr, 0, 0, 0};
-    k_tile_pass<<<static_cast<unsigned>(grid), NT, kSmemTotal, s>>>(none, d_work, n_work, total_tiles, d_passes,
-                                                                     d_phases, d_ops, d_mats, has_tc, err);
+    const TileWork none{nullptr, 0, nullptr, nullptr, nullptr, nullptr, 0, 0};
+    launch_tile_kernel(static_cast<unsigned>(grid), none, d_work, n_work, total_tiles, features, err, s);
     return cudaGetLastError();
 }
 

@@ -77,6 +77,8 @@ __host__ __device__ constexpr uint32_t reg_pair_index(uint32_t a, uint32_t b) { 
 // One register-level op, 64 bytes (four 16-byte words read with vector loads).
 //   TOP_DIAG: data = float2 offset of its tables in the matrix buffer:
 //     [flags & 1] R: 32 float2, the factor of each register index (terms on register bits only)
+//     [flags & 2] 256 float2, the factor of each thread (terms on the phase's thread bits only)
+//     [flags & 4] 256 u32, the sign pattern of each thread (pi terms: register x thread bits)
 //     n & 0xFFFF  T terms, 32 B each: {u64 mem mask, float2 p1, float2 p0}: a thread whose
 //                 index has every mask bit set multiplies by p1, otherwise by p0
 //     n >> 16     S terms, 16 B each: {u64 mem mask, u32 register pattern, 0}: sign flips
@@ -106,7 +108,7 @@ struct TilePass {
     uint8_t tile_pos[kTileQubits];    // tile-local position j -> memory qubit (ascending)
     uint8_t n_out;                    // number of non-tile qubits
     uint8_t n_low;                    // tile_pos[j] == j for j < n_low (>= 5): TMA chunk = 2^n_low amps
-    uint8_t has_tc;                   // the pass uses tensor-core ops
+    uint8_t has_tc;                   // kernel features the pass needs (kPassTensorCores | kPassWide)
     uint8_t out_mem[40];              // non-tile memory qubits, ascending
     uint32_t phase_begin, phase_end;
 };
@@ -125,19 +127,31 @@ struct TileProgram {
 struct TileWork {
     float2* state;
     uint64_t tile_begin;
-    uint32_t pass;
+    const TilePass* passes;     // the entry's program (its own arrays: states of
+    const TilePhase* phases;    // different programs share one launch)
+    const TileOp* ops;
+    const float2* mats;
+    uint32_t pass;              // index into `passes`
     uint32_t pad;
 };
 
+// Kernel features of a pass: tensor-core ops (the CTA allocates tensor
+// memory) and multi-qubit ops (SWAP, U2, DENSE: the larger kernel body).
+constexpr int kPassTensorCores = 1;
+constexpr int kPassWide = 2;
+
 // `err` (device int) receives a nonzero code if a bounded wait gave up.
-// `has_tc`: the pass contains TOP_DENSE_TC ops (the CTA allocates tensor memory).
+// `features`: the pass's kPass* bits (union over the entries of a work list).
 cudaError_t launch_tile_pass(float2* state, uint32_t n, const TilePass* d_passes, const TilePhase* d_phases,
-                             const TileOp* d_ops, const float2* d_mats, uint32_t pass_index, int has_tc,
+                             const TileOp* d_ops, const float2* d_mats, uint32_t pass_index, int features,
                              int* err, cudaStream_t s);
-// One launch over a work list in device memory (batched and served states).
-cudaError_t launch_tile_work(const TileWork* d_work, uint32_t n_work, uint64_t total_tiles, const TilePass* d_passes,
-                             const TilePhase* d_phases, const TileOp* d_ops, const float2* d_mats, int has_tc,
-                             int* err, cudaStream_t s);
+// Sets the tile kernel's shared-memory limit (once per process; call before
+// capturing a launch into a CUDA graph).
+cudaError_t configure_tile_kernel();
+// One launch over a work list in device memory (batched and served states);
+// `max_ctas` caps the grid (0: one CTA per SM).
+cudaError_t launch_tile_work(const TileWork* d_work, uint32_t n_work, uint64_t total_tiles, int features, int* err,
+                             cudaStream_t s, uint32_t max_ctas = 0);
 
 // Host-side helpers shared between engine.cpp and tile.cpp.
 struct Layout {

@@ -45,6 +45,7 @@ def emulate(plan, init=None):
             tp = P["tile_pos"]
             for ph in P["phases"]:
                 mq = [tp[r] for r in ph["reg_pos"]]
+                tq = [tp[r] for r in ph["thr_pos"]]
                 for op in ph["ops"]:
                     cmask = int(op["ctrl_mem"])
                     for j in range(5):
@@ -75,7 +76,7 @@ def emulate(plan, init=None):
                     elif kd == TOP_DENSE_TC:
                         apply_k(st, n, mq[:5], decode_tc_flat(plan, op["data"]), 0)
                     elif kd == TOP_DIAG:
-                        apply_diag(st, n, mq, op, words)
+                        apply_diag(st, n, mq, op, words, tq)
                     elif kd == TOP_CPHASE:
                         idx = np.arange(1 << n, dtype=np.int64)
                         sel = (idx & cmask) == cmask
@@ -99,13 +100,17 @@ def emulate(plan, init=None):
     return st
 
 
-def apply_diag(st, n, mq, op, words):
-    """TOP_DIAG: R table over the register index, T terms (thread/memory
-    masks, p1 where all set else p0), S sign terms, G general mixed terms."""
+def apply_diag(st, n, mq, op, words, tq):
+    """TOP_DIAG: R table over the register index, per-thread factor and sign
+    tables over the thread index, T terms (thread/memory masks, p1 where all
+    set else p0), S sign terms, G general mixed terms."""
     idx = np.arange(1 << n, dtype=np.int64)
     reg = np.zeros(idx.shape, dtype=np.int64)
     for j in range(5):
         reg |= ((idx >> mq[j]) & 1) << j
+    thr = np.zeros(idx.shape, dtype=np.int64)
+    for j in range(8):
+        thr |= ((idx >> tq[j]) & 1) << j
     w = words[2 * op["data"]:].astype(np.uint64)
     f = words[2 * op["data"]:].view(np.float32).astype(np.float64)
     pos = 0
@@ -114,6 +119,14 @@ def apply_diag(st, n, mq, op, words):
         R = f[0:64:2] + 1j * f[1:64:2]
         fac *= R[reg]
         pos = 64
+    if op["flags"] & 2:
+        Tt = f[pos:pos + 512:2] + 1j * f[pos + 1:pos + 512:2]
+        fac *= Tt[thr]
+        pos += 512
+    if op["flags"] & 4:
+        St = w[pos:pos + 256].astype(np.int64)
+        fac[((St[thr] >> reg) & 1) == 1] *= -1.0
+        pos += 256
     n_t, n_s, n_g = op["n"] & 0xFFFF, op["n"] >> 16, op["ctrl_reg"]
     for _ in range(n_t):
         c = int(w[pos]) | (int(w[pos + 1]) << 32)
