@@ -804,6 +804,17 @@ private:
     // as one TOP_DIAG op in phase `pb`.  With an accumulator (tensor-core
     // mode) register-only terms join it instead; every pending term commutes
     // with the accumulator's contents.
+    std::vector<HostOp> rot_buf_;   // commuting 1-qubit rotations awaiting emission
+    uint32_t rot_bits_ = 0;          // their register bits
+
+    void flush_rotations() {
+        std::stable_sort(rot_buf_.begin(), rot_buf_.end(),
+                         [](const HostOp& a, const HostOp& b) { return a.kind < b.kind; });
+        for (const HostOp& h : rot_buf_) emit_cuda_op(h);
+        rot_buf_.clear();
+        rot_bits_ = 0;
+    }
+
     void flush_pending(const PhaseBuild& pb, const int* local_of, Acc* acc, bool global) {
         cd R[32];
         for (cd& z : R) z = cd(1.0, 0.0);
@@ -1001,10 +1012,29 @@ private:
                 }
                 continue;
             }
-            if (pend_qubits_ & m.targets) flush_pending(pb, local_of, tc ? &acc : nullptr, false);
+            if (pend_qubits_ & m.targets) {
+                flush_rotations();
+                flush_pending(pb, local_of, tc ? &acc : nullptr, false);
+            }
             for (HostOp& h : host_ops(pb, local_of, m)) {
                 if (!tc) {
-                    emit_cuda_op(h);
+                    // Uncontrolled 1-qubit rotations on distinct register bits
+                    // commute: collect them and emit them grouped by kind, so
+                    // the kernel sees long runs of one kind.
+                    const bool rot = (h.kind == TOP_U1R || h.kind == TOP_RX || h.kind == TOP_U1) && h.cm == 0 &&
+                                     h.cmem == 0;
+                    if (rot && !(rot_bits_ & (1u << h.r0))) {
+                        rot_bits_ |= 1u << h.r0;
+                        rot_buf_.push_back(std::move(h));
+                        continue;
+                    }
+                    flush_rotations();
+                    if (rot) {
+                        rot_bits_ |= 1u << h.r0;
+                        rot_buf_.push_back(std::move(h));
+                    } else {
+                        emit_cuda_op(h);
+                    }
                     continue;
                 }
                 if (h.cmem == 0) {                       // uniform over the tile: fusable
@@ -1017,6 +1047,7 @@ private:
                 }
             }
         }
+        flush_rotations();
         if (last_phase) flush_pending(pb, local_of, tc ? &acc : nullptr, true);
         if (tc) flush(acc);
     }

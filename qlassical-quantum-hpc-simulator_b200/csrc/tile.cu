@@ -552,7 +552,34 @@ __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, co
             default: break;
             }
         } else {
-            switch (q0.x & 0xFFFFu) {
+            // Runs of uncontrolled rotations of one kind are applied by a
+            // loop over a 5-way switch: its merge points are cheaper than
+            // the full dispatch's.
+            uint32_t code = q0.x & 0xFFFFu;
+            if (code - OPC_U1R < 5u || code - OPC_RX < 5u) {
+                const uint32_t base = code - OPC_U1R < 5u ? OPC_U1R : OPC_RX;
+                for (;;) {
+                    if (base == OPC_U1R) {
+                        switch (code) {
+                            QLB_U1R_CASE(0) QLB_U1R_CASE(1) QLB_U1R_CASE(2) QLB_U1R_CASE(3) QLB_U1R_CASE(4)
+                        default: break;
+                        }
+                    } else {
+                        switch (code) {
+                            QLB_RX_CASE(0) QLB_RX_CASE(1) QLB_RX_CASE(2) QLB_RX_CASE(3) QLB_RX_CASE(4)
+                        default: break;
+                        }
+                    }
+                    if (oi + 1 >= ph.op_end) break;
+                    const uint4 nx = rec[4 * (oi + 1)];
+                    const uint32_t nc = nx.x & 0xFFFFu;
+                    if (nc - base >= 5u || (nx.y & 0x00FF0000u)) break;
+                    ++oi;
+                    code = nc;
+                }
+                continue;
+            }
+            switch (code) {
                 QLB_COMMON_CASES
             default: break;
             }
