@@ -300,6 +300,53 @@ int qlb_batch_stats(qlb_batch_t b, qlb_batch_info* out);
 int qlb_batch_stream(qlb_batch_t b, void** out_cuda_stream);
 int qlb_batch_destroy(qlb_batch_t b);
 
+/* ------------------------------------------------------------------------ */
+/* Serving loop: continuous batching of independent requests on one GPU.   */
+/* No counterpart in the reference.  A request = (circuit, shots, seed)    */
+/* run from |0...0>; its result = <Z_i> (FP64) and `shots` basis-state     */
+/* samples (counter-based, keyed by (seed, shot)).  Requests are admitted  */
+/* in arrival order while their state vector, program and sampling scratch */
+/* fit in a device arena reserved at creation, and join the running rounds */
+/* at the next round boundary (one tile pass per request per round).  A    */
+/* request's results do not depend on which requests share its rounds.    */
+/* ------------------------------------------------------------------------ */
+
+typedef struct qlb_server* qlb_server_t;
+
+typedef struct qlb_server_config {
+    uint64_t memory_bytes;  /* device arena; 0 = 85% of the free HBM at creation */
+    int      mode;          /* QLB_MODE_TILED (default) or QLB_MODE_TILED_TC */
+    uint32_t max_active;    /* admitted requests at once; 0 = 4096 */
+} qlb_server_config;
+
+typedef struct qlb_server_info {
+    uint64_t submitted, completed, rounds, launches, tiles;
+    uint32_t queued, active;
+    uint64_t arena_bytes, arena_used;
+} qlb_server_info;
+
+typedef struct qlb_request_info {
+    uint32_t num_qubits, passes;
+    uint64_t shots;
+    double   t_submit, t_admit, t_done;   /* seconds since the server started */
+} qlb_request_info;
+
+int qlb_server_create(qlb_server_t* out, const qlb_server_config* cfg);
+/* Plans the circuit on the calling thread and queues it (gates only, 1..30
+ * qubits); QLB_ERR_OOM if it can never fit the arena. */
+int qlb_server_submit(qlb_server_t s, const qlb_gate_instr* program, uint64_t count,
+                      const qlb_pool_view* pool, uint32_t num_qubits, uint64_t shots,
+                      uint64_t seed, uint64_t* out_request_id);
+/* Blocks until the request finished (QLB_ERR_TIMEOUT after timeout_s). */
+int qlb_server_wait(qlb_server_t s, uint64_t request_id, double timeout_s);
+/* Copies a finished request's results (either pointer may be NULL) and
+ * forgets the request. */
+int qlb_server_result(qlb_server_t s, uint64_t request_id, double* expect_z, uint32_t num_qubits,
+                      uint64_t* samples, uint64_t shots, qlb_request_info* info);
+int qlb_server_stats(qlb_server_t s, qlb_server_info* out);
+/* Finishes every submitted request, then stops the server thread. */
+int qlb_server_destroy(qlb_server_t s);
+
 #ifdef __cplusplus
 }
 #endif

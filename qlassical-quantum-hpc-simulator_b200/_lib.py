@@ -102,6 +102,25 @@ class BatchInfo(ctypes.Structure):
     ]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("memory_bytes", ctypes.c_uint64), ("mode", ctypes.c_int), ("max_active", ctypes.c_uint32)]
+
+
+class ServerInfo(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("rounds", ctypes.c_uint64),
+        ("launches", ctypes.c_uint64), ("tiles", ctypes.c_uint64), ("queued", ctypes.c_uint32),
+        ("active", ctypes.c_uint32), ("arena_bytes", ctypes.c_uint64), ("arena_used", ctypes.c_uint64),
+    ]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [
+        ("num_qubits", ctypes.c_uint32), ("passes", ctypes.c_uint32), ("shots", ctypes.c_uint64),
+        ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double),
+    ]
+
+
 class TranspileConfig(ctypes.Structure):
     _fields_ = [
         ("enable_gate_fusion", ctypes.c_int),
@@ -173,6 +192,12 @@ _SIGNATURES = {
     "qlb_batch_stats": [_P, ctypes.POINTER(BatchInfo)],
     "qlb_batch_stream": [_P, ctypes.POINTER(_P)],
     "qlb_batch_destroy": [_P],
+    "qlb_server_create": [ctypes.POINTER(_P), ctypes.POINTER(ServerConfig)],
+    "qlb_server_submit": [_P, _P, _U64, ctypes.POINTER(PoolView), _U32, _U64, _U64, _PU64],
+    "qlb_server_wait": [_P, _U64, ctypes.c_double],
+    "qlb_server_result": [_P, _U64, _P, _U32, _P, _U64, ctypes.POINTER(RequestInfo)],
+    "qlb_server_stats": [_P, ctypes.POINTER(ServerInfo)],
+    "qlb_server_destroy": [_P],
 }
 _OPTIONAL = {
     "qlb_transpile_gpu": [_P, _U64, ctypes.POINTER(PoolView), _U32, ctypes.POINTER(TranspileConfig),

@@ -10,6 +10,9 @@ float32, as the reference builder does (frontend.hpp:280-292).
   hea                hardware-efficient ansatz layer (RY, RZ, CZ ladder)
   hea_batch          the batched workload: HEA circuits with log-uniform
                      sizes in [10, 20] qubits and depths U{8..32}
+  serving_requests   the served workload: random_h_rx_cx circuits with
+                     log-uniform sizes in [12, 30] qubits, depths U{10..40}
+  poisson_arrivals   request arrival times of a Poisson process
   clustered          the reference benchmark's clustered H + CX-chain circuit
                      (benchmarks/bench_hw_awareness.cpp:30-53)
 """
@@ -107,6 +110,23 @@ def hea_batch(count: int = 4096, seed: int = 2024, n_min: int = 10, n_max: int =
     ds = rng.integers(d_min, d_max + 1, size=count)
     seeds = rng.integers(0, 2**31 - 1, size=count)
     return [hea(int(n), int(d), int(sd)) for n, d, sd in zip(ns, ds, seeds)]
+
+
+def serving_requests(count: int, seed: int = 7, n_min: int = 12, n_max: int = 30, d_min: int = 10,
+                     d_max: int = 40) -> list[IRModule]:
+    """The served workload: the H/RX + CX-ladder recipe of random_h_rx_cx
+    with n = round(exp(U[ln n_min, ln n_max])) and `layers` ~ U{d_min..d_max}."""
+    rng = np.random.default_rng(seed)
+    ns = np.rint(np.exp(rng.uniform(math.log(n_min), math.log(n_max), size=count))).astype(int)
+    ds = rng.integers(d_min, d_max + 1, size=count)
+    seeds = rng.integers(0, 2**31 - 1, size=count)
+    return [random_h_rx_cx(int(n), int(d), int(sd)) for n, d, sd in zip(ns, ds, seeds)]
+
+
+def poisson_arrivals(count: int, rate_hz: float, seed: int = 11) -> np.ndarray:
+    """Arrival times (seconds) of a Poisson process with the given rate."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate_hz, size=count))
 
 
 def expect_z_of(state: np.ndarray, n: int) -> np.ndarray:

@@ -145,6 +145,8 @@ constexpr int kPassWide = 2;
 cudaError_t launch_tile_pass(float2* state, uint32_t n, const TilePass* d_passes, const TilePhase* d_phases,
                              const TileOp* d_ops, const float2* d_mats, uint32_t pass_index, int features,
                              int* err, cudaStream_t s);
+int sm_count();   // multiprocessors of the current device (cached)
+
 // Sets the tile kernel's shared-memory limit (once per process; call before
 // capturing a launch into a CUDA graph).
 cudaError_t configure_tile_kernel();
