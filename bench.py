@@ -10,6 +10,8 @@ gates, so fusion and tiling count as speed).
 
   python bench.py [--gpus N --steps K --warmup W]      our engine (N replicas)
   python bench.py --impl reference                     the reference CPU engine
+  python bench.py --workload batched                   4096 HEA circuits per batch (circuits/s)
+  python bench.py --workload serving                   Poisson-arriving requests (p99 latency)
 
 Under torchrun each rank runs an independent replica on its own GPU (the
 path does not shard: "replicas only"); `value` is the sum over ranks of
@@ -33,6 +35,13 @@ sys.path.insert(0, ROOT)
 METRIC = "amp-updates/s"
 UNIT = "amp-updates/s"
 
+# DRAM bytes (read + write) of one tile pass per algorithmic byte (16 B per
+# amplitude), from one ncu capture of a 26-qubit pass (profiles/
+# k_tile_pass_26q_depth8.md: 1015.0 MB over 1073.7 MB); a pass's traffic
+# grows in proportion to the amplitudes it processes, so full-size launches
+# are scaled by this ratio.
+TRAFFIC_PER_ALGORITHMIC_BYTE = 1015.0 / 1073.7
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -46,6 +55,10 @@ def parse():
     ap.add_argument("--mode", default="tiled")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--workload", default="circuit", choices=["circuit", "batched", "serving"])
+    ap.add_argument("--circuits", type=int, default=4096, help="batched: circuits per batch")
+    ap.add_argument("--requests", type=int, default=200, help="serving: requests")
+    ap.add_argument("--rate", type=float, default=20.0, help="serving: Poisson arrival rate (1/s)")
     return ap.parse_args()
 
 
@@ -287,7 +300,8 @@ def run_ours(args):
         "config": config_of(args, module, extra),
         "hbm_gbs": hbm_gbs,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": TRAFFIC_PER_ALGORITHMIC_BYTE * bytes_per_launch,
+                     "traffic_source": "ncu dram bytes of a 26-qubit pass, scaled to 2^n amplitudes",
                      "kernel": "k_tile_pass", "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"},
         "clocks": clocks,
         "gpu_launches": args.steps * pstats["launches"],
@@ -309,10 +323,215 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def _peak_hbm():
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0))
+    except OSError:
+        return 6650.0
+
+
+def run_batched(args):
+    """Batched workload: `--circuits` HEA circuits (n log-uniform in [10, 20],
+    depth U{8..32}); a step = one run of the whole batch (|0...0> set-up, all
+    circuits, FP64 <Z_i>, results to pinned host memory) as one graph launch."""
+    import numpy as np
+    import torch
+    from __graft_entry__ import package
+    q = package()
+    from qlassical_b200 import circuits
+    from qlassical_b200.batch import Batch
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    q.engine.set_device(local)
+    mods = circuits.hea_batch(args.circuits, seed=2024)
+    mode = args.mode if args.mode in ("tiled", "tiled_tc", "auto") else "tiled"
+    t0 = time.perf_counter()
+    b = Batch(mods, mode)
+    build_s = time.perf_counter() - t0
+    st = b.stats()
+    stream = torch.cuda.ExternalStream(b.stream())
+    for _ in range(args.warmup):
+        b.run()
+    b.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            starts[i].record(stream)
+            b.run()
+            ends[i].record(stream)
+        b.synchronize()
+    total_ms = sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends))
+    step_s = total_ms / 1e3 / args.steps
+    value = world * len(mods) / step_s
+    ez = b.expect_z()
+    del b
+    # e2e: the public call with host programs: plan + upload + run + <Z> back
+    h2d = sum(m.program().nbytes + m.unitaries().data.nbytes for m in mods)
+    d2h = sum(8 * m.num_qubits for m in mods)
+    t0 = time.perf_counter()
+    from qlassical_b200.batch import run_batch
+    ez2 = run_batch(mods, mode)
+    e2e_s = time.perf_counter() - t0
+    assert all(np.array_equal(x, y) for x, y in zip(ez, ez2))
+    # sequential plain launches: one engine per size, one circuit at a time
+    sample = mods[:256]
+    engines = {}
+    t0 = time.perf_counter()
+    for m in sample:
+        eng = engines.get(m.num_qubits)
+        if eng is None:
+            eng = engines[m.num_qubits] = q.CUDAEngine(m.num_qubits, mode="plain")
+        eng.reset()
+        eng.execute(m)
+        eng.expect_z()
+    seq_plain = len(sample) / (time.perf_counter() - t0)
+    engines.clear()
+    # roofline: every tile pass reads and writes 16 B per amplitude
+    bytes_step = st["tiles"] * 8192 * 16.0
+    achieved = bytes_step / step_s / 1e9
+    peak = _peak_hbm()
+    line = {
+        "metric": "circuits/s", "value": value, "unit": "circuits/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64 (fp32)", "data": "synthetic",
+        "config": {"workload": f"{len(mods)} HEA circuits (RY,RZ per qubit + CZ ladder), n log-uniform in "
+                               f"[10, 20], depth U{{8..32}}, <Z_i> per circuit",
+                   "circuits": len(mods), "mode": st["mode"], "rounds": st["rounds"], "passes": st["passes"],
+                   "amp_updates_per_step": st["amp_updates"], "state_bytes": st["state_bytes"],
+                   "build_s": build_s, "l2": "4 GB of states, larger than the 126 MB L2"},
+        "amp_updates_per_s": st["amp_updates"] / step_s,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": TRAFFIC_PER_ALGORITHMIC_BYTE * bytes_step / max(1, st["rounds"]),
+                     "traffic_source": "ncu dram bytes of a 26-qubit pass, scaled to the tiles of a round",
+                     "kernel": "k_tile_pass (all rounds)",
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"},
+        "sequential_plain": {"value": seq_plain, "unit": "circuits/s",
+                             "sample": "first 256 circuits, CUDAEngine plain mode, one circuit at a time"},
+        "clocks": clk.summary(),
+        "gpu_launches": args.steps * st["launches"],
+        "e2e": {"value": len(mods) / e2e_s, "unit": "circuits/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            from oracle import oracle
+            from qlassical_b200.ir import IRModule, UnitaryPool
+            sub = mods[:32]
+            t = 0.0
+            for m in sub:
+                prog, data, meta = oracle.transpile_reference(circuits.to_reference_ir(m))   # untimed, as the
+                ref = IRModule(m.num_qubits, unitary_pool=UnitaryPool.from_arrays(data, meta))  # reference's
+                ref.set_program(prog)                                                        # benchmark loop
+                t += oracle.time_reference(ref, reps=1)
+            line["cpu_baseline"] = {"value": len(sub) / t, "unit": "circuits/s", "cores": oracle.reference_threads(),
+                                    "kind": "reference",
+                                    "sample": f"first {len(sub)} circuits, reference fusion k<=4, CPUOpenMPEngine"}
+        except Exception as ex:
+            line["cpu_baseline"] = {"value": None, "unit": "circuits/s", "cores": None, "kind": "reference",
+                                    "sample": f"unavailable: {ex}"}
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def run_serving(args):
+    """Serving workload: `--requests` requests (random_h_rx_cx recipe, n
+    log-uniform in [12, 30], depth U{10..40}, 1024 shots + <Z_i> each)
+    arriving as a Poisson process of rate `--rate`; latency = finish - submit."""
+    import numpy as np
+    import torch
+    from __graft_entry__ import package
+    q = package()
+    from qlassical_b200 import circuits
+    from qlassical_b200.serve import Server
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    q.engine.set_device(local)
+    mods = circuits.serving_requests(args.requests, seed=7)
+    arrivals = circuits.poisson_arrivals(args.requests, args.rate, seed=11)
+    srv = Server()
+    # warm-up: a few small requests (kernel set-up, first launches)
+    for m in circuits.serving_requests(4, seed=99, n_max=14):
+        srv.result(srv.submit(m, shots=16, seed=1))
+    ids = [0] * len(mods)
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for i, m in enumerate(mods):
+            delay = arrivals[i] - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            ids[i] = srv.submit(m, shots=1024, seed=i)
+        res = [srv.result(i) for i in ids]
+    stats = srv.stats()
+    srv.close()
+    lat = np.array([r.latency for r in res])
+    ns = np.array([m.num_qubits for m in mods])
+    span = max(r.t_done for r in res) - min(r.t_submit for r in res)
+    gates = np.array([m.gate_count() for m in mods], dtype=np.float64)
+    amp_updates = float(np.sum(gates * np.exp2(ns)))
+    # sequential plain launches: service time per request from plain-mode
+    # rates measured at two sizes, queued one at a time on the same arrivals
+    rates = {}
+    for n_probe in (16, 24):
+        m = circuits.random_h_rx_cx(n_probe, 10, seed=3)
+        eng = q.CUDAEngine(n_probe, mode="plain")
+        eng.execute(m)
+        eng.synchronize()
+        t_ = time.perf_counter()
+        eng.reset()
+        eng.execute(m)
+        eng.expect_z()
+        eng.sample(1, 1024)
+        rates[n_probe] = m.gate_count() * float(1 << n_probe) / (time.perf_counter() - t_)
+        del eng
+    done = 0.0
+    seq_lat = []
+    for i, m in enumerate(mods):
+        rate = rates[16] if m.num_qubits < 20 else rates[24]
+        svc = m.gate_count() * float(1 << m.num_qubits) / rate
+        start = max(arrivals[i], done)
+        done = start + svc
+        seq_lat.append(done - arrivals[i])
+    seq_lat = np.array(seq_lat)
+    h2d = sum(m.program().nbytes for m in mods)
+    d2h = sum(8 * m.num_qubits + 8 * 1024 for m in mods)
+    p99 = float(np.percentile(lat, 99))
+    line = {
+        "metric": "request latency p99", "value": p99, "unit": "s", "n_gpus": 1, "steps": len(mods),
+        "warmup": 4, "ms_per_step": 1e3 * span / len(mods), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64 (fp32)", "data": "synthetic",
+        "config": {"workload": f"{len(mods)} requests, Poisson arrivals at {args.rate}/s, random H/RX + CX-ladder "
+                               f"circuits, n log-uniform in [12, 30], depth U{{10..40}}, 1024 shots + <Z_i>",
+                   "requests": len(mods), "rate_hz": args.rate, "lanes": "small (<22 qubits) / large, SM-partitioned"},
+        "p50_s": float(np.percentile(lat, 50)), "p99_s": p99, "mean_s": float(lat.mean()),
+        "p50_small_s": float(np.percentile(lat[ns < 22], 50)),
+        "p50_large_s": float(np.percentile(lat[ns >= 22], 50)) if np.any(ns >= 22) else None,
+        "circuits_per_s": len(mods) / span, "amp_updates_per_s": amp_updates / span,
+        "server": stats,
+        "sequential_plain": {"p50_s": float(np.percentile(seq_lat, 50)), "p99_s": float(np.percentile(seq_lat, 99)),
+                             "circuits_per_s": len(mods) / max(1e-9, done - arrivals[0]),
+                             "method": "plain-mode service times from rates measured at 16 and 24 qubits, "
+                                       "queued one request at a time on the same arrivals (modelled)"},
+        "clocks": clk.summary(),
+        "gpu_launches": int(stats["launches"]),
+        "e2e": {"value": p99, "unit": "s", "h2d_bytes_per_step": int(h2d / len(mods)),
+                "d2h_bytes_per_step": int(d2h / len(mods))},
+    }
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batched":
+        run_batched(args)
+    elif args.workload == "serving":
+        run_serving(args)
     else:
         run_ours(args)
 
