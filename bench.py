@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--workload", default="circuit", choices=["circuit", "batched", "serving"])
+    ap.add_argument("--circuit", default="rot_cz", choices=["rot_cz", "qft"],
+                    help="circuit workload: random rotations + CZ (default) or the QFT of |0...0>")
     ap.add_argument("--circuits", type=int, default=4096, help="batched: circuits per batch")
     ap.add_argument("--requests", type=int, default=200, help="serving: requests")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: Poisson arrival rate (1/s)")
@@ -64,12 +66,16 @@ def parse():
 
 def workload(args):
     from qlassical_b200 import circuits
+    if args.circuit == "qft":
+        return circuits.qft(args.qubits)
     return circuits.random_rot_cz(args.qubits, args.depth, seed=args.seed)
 
 
 def config_of(args, module, extra=None):
+    name = (f"QFT (H + CP ladders + bit-reversal swaps), {args.qubits} qubits" if args.circuit == "qft" else
+            f"random RX/RY/RZ + CZ-pairs circuit, {args.qubits} qubits, depth {args.depth}")
     c = {
-        "workload": f"random RX/RY/RZ + CZ-pairs circuit, {args.qubits} qubits, depth {args.depth}",
+        "workload": name,
         "n_qubits": args.qubits,
         "depth": args.depth,
         "seed": args.seed,

@@ -222,6 +222,10 @@ int qlb_expect_z_noalloc(const void* state_float2, uint32_t num_qubits, double* 
 /* Draws `shots` basis states from |amp|^2 with a counter-based generator
  * keyed by `seed`; identical seeds give identical samples on any launch. */
 int qlb_engine_sample(qlb_engine_t e, uint64_t seed, uint64_t shots, uint64_t* out);
+/* Amplitudes at chosen indices (complex128, `count` of them): a device-side
+ * gather, for states too large to download (the reference's state() view
+ * has no GPU equivalent at 33 qubits). */
+int qlb_engine_amplitudes_at(qlb_engine_t e, const uint64_t* indices, uint64_t count, double* out_c128);
 
 /* ------------------------------------------------------------------------ */
 /* GPU middle end (replaces Middleware::transpile_gpu, middleware.hpp:866)  */

@@ -179,6 +179,7 @@ _SIGNATURES = {
     "qlb_engine_prob_one": [_P, _U32, _PD],
     "qlb_engine_expect_z": [_P, _P, _U32],
     "qlb_engine_sample": [_P, _U64, _U64, _P],
+    "qlb_engine_amplitudes_at": [_P, _P, _U64, _P],
     "qlb_engine_set_option": [_P, _I, ctypes.c_int64],
     "qlb_engine_compile": [_P, _P, _U64, ctypes.POINTER(PoolView), ctypes.POINTER(_P)],
     "qlb_engine_run": [_P, _P],

@@ -729,6 +729,25 @@ int qlb_engine_expect_z(qlb_engine_t e, double* out, uint32_t nq) {
     });
 }
 
+int qlb_engine_amplitudes_at(qlb_engine_t e, const uint64_t* indices, uint64_t count, double* out_c128) {
+    return guarded([&] {
+        need(e, "engine");
+        if (count && (!indices || !out_c128)) fail(QLB_ERR_INVALID_ARG, "indices / out is null");
+        if (e->sv.dim == 0) fail(QLB_ERR_STATE, "engine has no state vector");
+        for (uint64_t i = 0; i < count; ++i)
+            if (indices[i] >= e->sv.dim) fail(QLB_ERR_INVALID_ARG, "amplitude index out of range");
+        if (count == 0) return;
+        char* buf = static_cast<char*>(e->staging.ensure(count * (sizeof(uint64_t) + 2 * sizeof(double)) + 256));
+        auto* d_idx = reinterpret_cast<uint64_t*>(buf);
+        auto* d_out = reinterpret_cast<double2*>(buf + ((count * sizeof(uint64_t) + 255) & ~size_t{255}));
+        check_cuda(cudaMemcpyAsync(d_idx, indices, count * sizeof(uint64_t), cudaMemcpyHostToDevice, e->stream), "H2D");
+        check_cuda(launch_gather(e->sv.d, d_idx, count, d_out, e->stream), "gather");
+        check_cuda(cudaMemcpyAsync(out_c128, d_out, count * 2 * sizeof(double), cudaMemcpyDeviceToHost, e->stream),
+                   "D2H");
+        check_cuda(cudaStreamSynchronize(e->stream), "gather sync");
+    });
+}
+
 int qlb_engine_sample(qlb_engine_t e, uint64_t seed, uint64_t shots, uint64_t* out) {
     return guarded([&] {
         need(e, "engine");

@@ -18,6 +18,8 @@ cudaError_t launch_init_zero(float2* a, uint64_t dim, cudaStream_t s);
 // complex128 (device staging) -> complex64 state slice
 cudaError_t launch_c128_to_c64(const double2* src, float2* dst, uint64_t count, cudaStream_t s);
 cudaError_t launch_c64_to_c128(const float2* src, double2* dst, uint64_t count, cudaStream_t s);
+// out[i] = a[idx[i]] widened to complex128 (idx checked by the caller).
+cudaError_t launch_gather(const float2* a, const uint64_t* idx, uint64_t count, double2* out, cudaStream_t s);
 
 // ---- plain per-instruction kernels (gates.cu) ---------------------------
 // Generic 2x2 on target t (one HBM sweep).

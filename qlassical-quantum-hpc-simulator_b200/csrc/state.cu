@@ -35,7 +35,21 @@ __global__ void k_c64_to_c128(const float2* __restrict__ src, double2* __restric
         dst[i] = make_double2(v.x, v.y);
     }
 }
+__global__ void k_gather(const float2* __restrict__ a, const uint64_t* __restrict__ idx, uint64_t count,
+                         double2* __restrict__ out) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < count; i += stride) {
+        const float2 v = a[idx[i]];
+        out[i] = make_double2(v.x, v.y);
+    }
+}
 }  // namespace
+
+cudaError_t launch_gather(const float2* a, const uint64_t* idx, uint64_t count, double2* out, cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    k_gather<<<sweep_grid(count, kThreads), kThreads, 0, s>>>(a, idx, count, out);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_init_zero(float2* a, uint64_t dim, cudaStream_t s) {
     if (dim == 0) return cudaErrorInvalidValue;

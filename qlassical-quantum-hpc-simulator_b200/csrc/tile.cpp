@@ -930,7 +930,30 @@ private:
             }
             S.swap(skeep);
         }
-        if (!has_r && ttab.empty() && stab.empty() && T.empty() && S.empty() && Gs.empty()) return;
+        // General mixed terms on thread bits: one per-thread factor table per
+        // distinct register mask (a CP between a register and a thread qubit).
+        std::vector<uint32_t> gcm;
+        std::vector<std::vector<cd>> gtab;
+        {
+            std::vector<G> gkeep;
+            for (const G& g : Gs) {
+                if ((g.cmem & ~thr_mask) != 0 || gcm.size() >= 255) {
+                    gkeep.push_back(g);
+                    continue;
+                }
+                size_t k = 0;
+                while (k < gcm.size() && gcm[k] != g.cm) ++k;
+                if (k == gcm.size()) {
+                    gcm.push_back(g.cm);
+                    gtab.emplace_back(256, cd(1.0, 0.0));
+                }
+                for (uint32_t th = 0; th < 256; ++th)
+                    if ((thread_bits(th) & g.cmem) == g.cmem) gtab[k][th] *= g.p1;
+            }
+            Gs.swap(gkeep);
+            std::stable_sort(Gs.begin(), Gs.end(), [](const G& a, const G& b) { return a.cm < b.cm; });
+        }
+        if (!has_r && ttab.empty() && stab.empty() && gcm.empty() && T.empty() && S.empty() && Gs.empty()) return;
         if (T.size() > 0xFFFF || S.size() > 0xFFFF) fail(QLB_ERR_INVALID_ARG, "too many diagonal terms in one pass");
         auto f2 = [](cd z) { return make_float2(static_cast<float>(z.real()), static_cast<float>(z.imag())); };
         auto words = [&](uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
@@ -950,7 +973,8 @@ private:
         op.kind = TOP_DIAG;
         op.code = OPC_DIAG;
         op.data = static_cast<uint32_t>(prog.mats.size());
-        op.flags = (has_r ? 1u : 0u) | (ttab.empty() ? 0u : 2u) | (stab.empty() ? 0u : 4u);
+        op.flags = (has_r ? 1u : 0u) | (ttab.empty() ? 0u : 2u) | (stab.empty() ? 0u : 4u) |
+                   (static_cast<uint32_t>(gcm.size()) << 8);
         op.n = static_cast<uint32_t>(T.size()) | (static_cast<uint32_t>(S.size()) << 16);
         op.ctrl_reg = static_cast<uint32_t>(Gs.size());
         if (has_r)
@@ -962,6 +986,11 @@ private:
             std::memcpy(&f.y, &stab[th + 1], 4);
             prog.mats.push_back(f);
         }
+        for (size_t k = 0; k < gcm.size(); k += 4)    // register masks, four per 16 bytes
+            words(gcm[k], k + 1 < gcm.size() ? gcm[k + 1] : 0u, k + 2 < gcm.size() ? gcm[k + 2] : 0u,
+                  k + 3 < gcm.size() ? gcm[k + 3] : 0u);
+        for (const auto& tab : gtab)
+            for (const cd& z : tab) prog.mats.push_back(f2(z));
         for (const PTerm& t : T) {
             const float2 a = f2(t.p1), b = f2(t.p0);
             words(static_cast<uint32_t>(t.mask), static_cast<uint32_t>(t.mask >> 32), bits(a.x), bits(a.y));

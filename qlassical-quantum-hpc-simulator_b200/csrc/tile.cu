@@ -423,6 +423,11 @@ __device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* __restric
         smask = __ldg(reinterpret_cast<const uint32_t*>(q) + threadIdx.x);
         q += 128;
     }
+    const uint32_t n_gt = (flags >> 8) & 0xFFu;
+    const uint32_t* gcm = reinterpret_cast<const uint32_t*>(q);
+    q += 2 * ((n_gt + 3) / 4);
+    const float2* gtab = q;
+    q += 256 * n_gt;
     const uint4* p = reinterpret_cast<const uint4*>(q);
 #pragma unroll 2
     for (uint32_t t = 0; t < n_t; ++t) {
@@ -456,15 +461,34 @@ __device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* __restric
             v[m].y = __uint_as_float(__float_as_uint(v[m].y) ^ sgn);
         }
     }
-    for (uint32_t g = 0; g < n_g; ++g) {
-        const uint4 w0 = __ldg(p + 2 * g), w1 = __ldg(p + 2 * g + 1);
-        const uint64_t c = (static_cast<uint64_t>(w0.y) << 32) | w0.x;
-        if ((gt & c) != c) continue;
-        const uint32_t cm = w0.z;
-        const float2 ph = make_float2(__uint_as_float(w1.x), __uint_as_float(w1.y));
+    for (uint32_t g = 0; g < n_gt; ++g) {
+        const float2 f = __ldg(gtab + 256 * g + threadIdx.x);
+        if (f.x == 1.f && f.y == 0.f) continue;
+        const uint32_t cm = __ldg(gcm + g);
 #pragma unroll
         for (int m = 0; m < NR; ++m)
-            if ((static_cast<uint32_t>(m) & cm) == cm) v[m] = cmul(v[m], ph);
+            if ((static_cast<uint32_t>(m) & cm) == cm) v[m] = cmul(v[m], f);
+    }
+    // G terms arrive grouped by register mask: the factors of a group are
+    // multiplied per thread, then applied once.
+    float2 gf = make_float2(1.f, 0.f);
+    uint32_t gcur = 0;
+    for (uint32_t g = 0; g <= n_g; ++g) {
+        uint4 w0 = make_uint4(0u, 0u, 0xFFFFFFFFu, 0u), w1 = make_uint4(0u, 0u, 0u, 0u);
+        if (g < n_g) {
+            w0 = __ldg(p + 2 * g);
+            w1 = __ldg(p + 2 * g + 1);
+        }
+        if (g > 0 && w0.z != gcur && (gf.x != 1.f || gf.y != 0.f)) {
+#pragma unroll
+            for (int m = 0; m < NR; ++m)
+                if ((static_cast<uint32_t>(m) & gcur) == gcur) v[m] = cmul(v[m], gf);
+        }
+        if (g == n_g) break;
+        if (w0.z != gcur || g == 0) gf = make_float2(1.f, 0.f);
+        gcur = w0.z;
+        const uint64_t c = (static_cast<uint64_t>(w0.y) << 32) | w0.x;
+        if ((gt & c) == c) gf = cmul(gf, make_float2(__uint_as_float(w1.x), __uint_as_float(w1.y)));
     }
 }
 

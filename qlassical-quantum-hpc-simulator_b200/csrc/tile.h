@@ -79,6 +79,8 @@ __host__ __device__ constexpr uint32_t reg_pair_index(uint32_t a, uint32_t b) { 
 //     [flags & 1] R: 32 float2, the factor of each register index (terms on register bits only)
 //     [flags & 2] 256 float2, the factor of each thread (terms on the phase's thread bits only)
 //     [flags & 4] 256 u32, the sign pattern of each thread (pi terms: register x thread bits)
+//     g = (flags >> 8) & 0xFF: g register masks (u32, padded to 16 B), then g tables of
+//                 256 float2: thread t multiplies the registers containing mask k by table k[t]
 //     n & 0xFFFF  T terms, 32 B each: {u64 mem mask, float2 p1, float2 p0}: a thread whose
 //                 index has every mask bit set multiplies by p1, otherwise by p0
 //     n >> 16     S terms, 16 B each: {u64 mem mask, u32 register pattern, 0}: sign flips

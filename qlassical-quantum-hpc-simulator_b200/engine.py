@@ -279,6 +279,14 @@ class CUDAEngine:
         call("qlb_engine_expect_z", self._h, _lib.ptr(out), n)
         return out
 
+    def amplitudes_at(self, indices) -> np.ndarray:
+        """Amplitudes at the given basis indices (device-side gather)."""
+        idx = np.ascontiguousarray(indices, dtype=np.uint64)
+        out = np.empty(idx.size, dtype=np.complex128)
+        call("qlb_engine_amplitudes_at", self._h, idx.ctypes.data if idx.size else None, idx.size,
+             out.ctypes.data if idx.size else None)
+        return out
+
     def sample(self, seed: int, shots: int) -> np.ndarray:
         out = np.empty(int(shots), dtype=np.uint64)
         call("qlb_engine_sample", self._h, int(seed) & 0xFFFFFFFFFFFFFFFF, int(shots), _lib.ptr(out))

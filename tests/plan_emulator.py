@@ -127,6 +127,15 @@ def apply_diag(st, n, mq, op, words, tq):
         St = w[pos:pos + 256].astype(np.int64)
         fac[((St[thr] >> reg) & 1) == 1] *= -1.0
         pos += 256
+    n_gt = (op["flags"] >> 8) & 0xFF
+    if n_gt:
+        cms = [int(c) for c in w[pos:pos + n_gt]]
+        pos += 4 * ((n_gt + 3) // 4)
+        for k in range(n_gt):
+            tab = f[pos:pos + 512:2] + 1j * f[pos + 1:pos + 512:2]
+            hit = (reg & cms[k]) == cms[k]
+            fac[hit] *= tab[thr[hit]]
+            pos += 512
     n_t, n_s, n_g = op["n"] & 0xFFFF, op["n"] >> 16, op["ctrl_reg"]
     for _ in range(n_t):
         c = int(w[pos]) | (int(w[pos + 1]) << 32)
