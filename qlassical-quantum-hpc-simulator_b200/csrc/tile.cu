@@ -29,7 +29,7 @@ constexpr uint32_t kWaitLimit = 1u << 26;
 constexpr size_t kSmemBuffers = 3 * TILE * sizeof(float2);   // 2 TMA buffers + 1 transpose buffer
 constexpr size_t kSmemOps = kMaxSmemOps * sizeof(TileOp);
 constexpr size_t kSmemPhases = kMaxSmemPhases * sizeof(TilePhase);
-constexpr size_t kSmemMisc = 64;             // 2 TMA mbarriers, MMA mbarrier, TMEM address
+constexpr size_t kSmemMisc = 64;             // 2 TMA mbarriers, MMA and B-copy mbarriers, TMEM address
 constexpr size_t kSmemTcB = 16384;           // B operand staging of a tensor-core op
 constexpr size_t kSmemTotal = kSmemBuffers + kSmemOps + kSmemPhases + sizeof(TilePass) + kSmemMisc + kSmemTcB;
 
@@ -295,9 +295,6 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t smem_addr) {
            (static_cast<uint64_t>(1024u >> 4) << 32) | (uint64_t{1} << 46);
 }
 
-__device__ __forceinline__ uint32_t bf16_bits_rn(float x) {
-    return static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16_rn(x)));
-}
 __device__ __forceinline__ float bf16_to_float(uint32_t b) { return __uint_as_float(b << 16); }
 
 // Writes this thread's row of A (hi and lo) into the canonical layout.
@@ -309,13 +306,17 @@ __device__ __forceinline__ void tc_write_a(const float2 (&v)[NR], unsigned char*
         uint32_t hi[4], lo[4];
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
+            // two reals per instruction: x -> hi = bf16(x), lo = bf16(x - hi)
             const int k0 = c * 8 + 2 * e;
             const float x0 = k0 < 32 ? v[k0].x : v[k0 - 32].y;
             const float x1 = (k0 + 1) < 32 ? v[k0 + 1].x : v[k0 + 1 - 32].y;
-            const uint32_t h0 = bf16_bits_rn(x0), h1 = bf16_bits_rn(x1);
-            const uint32_t l0 = bf16_bits_rn(x0 - bf16_to_float(h0)), l1 = bf16_bits_rn(x1 - bf16_to_float(h1));
-            hi[e] = h0 | (h1 << 16);
-            lo[e] = l0 | (l1 << 16);
+            const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+            const uint32_t hb = *reinterpret_cast<const uint32_t*>(&h);
+            const float2 r = __fadd2_rn(make_float2(x0, x1),
+                                        make_float2(-bf16_to_float(hb & 0xFFFFu), -__uint_as_float(hb & 0xFFFF0000u)));
+            const __nv_bfloat162 l = __floats2bfloat162_rn(r.x, r.y);
+            hi[e] = hb;
+            lo[e] = *reinterpret_cast<const uint32_t*>(&l);
         }
         *reinterpret_cast<uint4*>(a_hi + rowoff + c * 128u) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
         *reinterpret_cast<uint4*>(a_lo + rowoff + c * 128u) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
@@ -360,8 +361,9 @@ __device__ __forceinline__ void tc_ld_row(uint32_t taddr, uint32_t (&r)[64]) {
 struct TcCtx {
     uint32_t tmem;        // TMEM base address (lane 0, column base)
     uint64_t* bar;        // MMA-completion mbarrier
+    uint64_t* bbar;       // B-operand copy mbarrier
     unsigned char* sb;    // 16 KB B staging area
-    uint32_t uses;        // completed TC ops of this CTA (mbarrier parity)
+    uint32_t uses;        // completed TC ops of this CTA (parity of both mbarriers)
 };
 
 // Applies one TC op; returns false if the MMA wait gave up (all threads agree).
@@ -369,17 +371,18 @@ __device__ __forceinline__ bool op_dense_tc(float2 (&v)[NR], const float2* __res
                                             TcCtx& tc) {
     unsigned char* a_hi = reinterpret_cast<unsigned char*>(cur);
     unsigned char* a_lo = a_hi + 32768;
-    // stage B (16 KB) while no one reads shared memory; everyone has read `cur`
-    __syncthreads();
-    {
-        const uint4* src = reinterpret_cast<const uint4*>(bimg);
-        uint4* dst = reinterpret_cast<uint4*>(tc.sb);
-        for (uint32_t i = threadIdx.x; i < kTcBBytes / 16; i += NT) dst[i] = __ldg(src + i);
+    // B (16 KB) arrives by a bulk async copy while the CTA converts A; the
+    // staging area is free: the previous TC op's MMAs have completed.
+    if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(tc.bbar, kTcBBytes);
+        bulk_g2s(tc.sb, bimg, kTcBBytes, tc.bbar);
     }
+    __syncthreads();          // everyone has read `cur`, which now receives A
     tc_write_a(v, a_hi, a_lo);
-    fence_proxy_async();      // generic writes of A and B -> visible to the tensor core
+    fence_proxy_async();      // generic writes of A -> visible to the tensor core
     tc_fence_before();
-    __syncthreads();
+    const bool okb = mbar_wait_bounded(tc.bbar, tc.uses & 1u);
+    if (__syncthreads_or(!okb)) return false;
     if (threadIdx.x == 0) {
         tc_fence_after();
         const uint32_t ahi = smem_u32(a_hi), alo = smem_u32(a_lo), bhi = smem_u32(tc.sb), blo = bhi + 8192u;
@@ -645,13 +648,14 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
     TilePhase* sph = reinterpret_cast<TilePhase*>(smem_raw + kSmemBuffers + kSmemOps);
     TilePass* spass = reinterpret_cast<TilePass*>(smem_raw + kSmemBuffers + kSmemOps + kSmemPhases);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + kSmemBuffers + kSmemOps + kSmemPhases + sizeof(TilePass));
-    uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(bar + 3);
+    uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(bar + 4);
     unsigned char* sb = smem_raw + kSmemBuffers + kSmemOps + kSmemPhases + sizeof(TilePass) + kSmemMisc;
 
     if (threadIdx.x == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
         mbar_init(&bar[2], 1);
+        mbar_init(&bar[3], 1);
         fence_mbar_init();
     }
     if (has_tc && threadIdx.x < 32) {     // warp 0 owns the tensor-memory allocation
@@ -663,7 +667,7 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    TcCtx tc{has_tc ? *tmem_holder : 0u, &bar[2], sb, 0u};
+    TcCtx tc{has_tc ? *tmem_holder : 0u, &bar[2], &bar[3], sb, 0u};
     bool failed = false;
 
     auto entry = [&](uint64_t t) -> TileWork { return n_work ? work[find_work(work, n_work, t)] : single; };
@@ -776,7 +780,10 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
         }
         __syncthreads();   // everyone is done with `cur` before it is refilled
     }
-    if (failed && has_tc) mbar_wait_bounded(&bar[2], tc.uses & 1u);   // a late MMA, if any
+    if (failed && has_tc) {   // a late MMA or B copy, if any
+        mbar_wait_bounded(&bar[2], tc.uses & 1u);
+        mbar_wait_bounded(&bar[3], tc.uses & 1u);
+    }
     tc_fence_before();
     __syncthreads();
     if (has_tc && threadIdx.x < 32) {
