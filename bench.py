@@ -56,8 +56,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--workload", default="circuit", choices=["circuit", "batched", "serving"])
-    ap.add_argument("--circuit", default="rot_cz", choices=["rot_cz", "qft"],
-                    help="circuit workload: random rotations + CZ (default) or the QFT of |0...0>")
+    ap.add_argument("--circuit", default="rot_cz", choices=["rot_cz", "qft", "fused"],
+                    help="circuit workload: random rotations + CZ (default), the same after k=5 fusion, or the QFT")
     ap.add_argument("--circuits", type=int, default=4096, help="batched: circuits per batch")
     ap.add_argument("--requests", type=int, default=200, help="serving: requests")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: Poisson arrival rate (1/s)")
@@ -65,15 +65,35 @@ def parse():
 
 
 def workload(args):
+    """The circuit of one step.  `fused` is the rotation circuit after the
+    GPU middle end (fusion into dense blocks of up to 5 qubits plus qubit
+    windowing), the form in which its dense blocks reach the tensor cores."""
     from qlassical_b200 import circuits
     if args.circuit == "qft":
         return circuits.qft(args.qubits)
+    m = circuits.random_rot_cz(args.qubits, args.depth, seed=args.seed)
+    if args.circuit == "fused":
+        from qlassical_b200.middleware import Middleware, TranspilerConfig
+        return Middleware().transpile(m, config=TranspilerConfig(max_fusion_qubits=5))
+    return m
+
+
+def circuits_rot_cz(args):
+    from qlassical_b200 import circuits
     return circuits.random_rot_cz(args.qubits, args.depth, seed=args.seed)
+
+
+def logical_gates(args, module):
+    """Gates before fusion (the amp-update count uses these)."""
+    if args.circuit == "fused":
+        return circuits_rot_cz(args).gate_count()
+    return module.gate_count()
 
 
 def config_of(args, module, extra=None):
     name = (f"QFT (H + CP ladders + bit-reversal swaps), {args.qubits} qubits" if args.circuit == "qft" else
-            f"random RX/RY/RZ + CZ-pairs circuit, {args.qubits} qubits, depth {args.depth}")
+            f"random RX/RY/RZ + CZ-pairs circuit, {args.qubits} qubits, depth {args.depth}"
+            + (", middle-end fusion k<=5 + windowing" if args.circuit == "fused" else ""))
     c = {
         "workload": name,
         "n_qubits": args.qubits,
@@ -219,7 +239,7 @@ def run_ours(args):
 
     module = workload(args)
     n = module.num_qubits
-    gates = module.gate_count()
+    gates = logical_gates(args, module)
     eng = q.CUDAEngine(n, seed=1, mode=args.mode)
     plan = eng.compile(module)
     pstats = plan.stats()
@@ -330,7 +350,9 @@ def run_ours(args):
         line["plain_gpu"] = plain
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = cpu_baseline(args, module, max_gates=45)
+            # the reference engine takes blocks of <= 4 qubits: it runs the unfused circuit
+            base = module if args.circuit != "fused" else circuits_rot_cz(args)
+            line["cpu_baseline"] = cpu_baseline(args, base, max_gates=45)
         except Exception as ex:  # the oracle libraries are test infrastructure
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
                                     "sample": f"unavailable: {ex}"}
