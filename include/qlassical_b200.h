@@ -101,6 +101,13 @@ const char* qlb_version(void);
  * inherited). */
 int qlb_set_device(int device);
 int qlb_device_info(int* sm_count, uint64_t* free_bytes, uint64_t* total_bytes);
+/* Failure-path self-test (no reference counterpart): runs the device wait
+ * that the tile kernel uses for copy and tensor-core completions on a
+ * barrier that nothing completes, with a limit of limit_ms (1..2000).  The
+ * wait must give up and report: *gave_up = 1, and the CUDA context stays
+ * usable.  Every wait of the tile kernel is bounded this way (2 s); when one
+ * gives up, the call that launched it returns QLB_ERR_TIMEOUT. */
+int qlb_selftest_bounded_wait(uint32_t limit_ms, int* gave_up);
 
 /* ------------------------------------------------------------------------ */
 /* CUDAStateVector (replaces CPUStateVector, cpu_state_vector.hpp:24-162)   */
@@ -341,8 +348,13 @@ int qlb_server_create(qlb_server_t* out, const qlb_server_config* cfg);
 int qlb_server_submit(qlb_server_t s, const qlb_gate_instr* program, uint64_t count,
                       const qlb_pool_view* pool, uint32_t num_qubits, uint64_t shots,
                       uint64_t seed, uint64_t* out_request_id);
-/* Blocks until the request finished (QLB_ERR_TIMEOUT after timeout_s). */
+/* Blocks until the request finished (QLB_ERR_TIMEOUT after timeout_s;
+ * QLB_ERR_STATE if it was cancelled). */
 int qlb_server_wait(qlb_server_t s, uint64_t request_id, double timeout_s);
+/* Cancels a request: a queued one leaves the queue at once, an admitted one
+ * at the next round boundary (its device memory is then released).  No
+ * effect on a finished request. */
+int qlb_server_cancel(qlb_server_t s, uint64_t request_id);
 /* Copies a finished request's results (either pointer may be NULL) and
  * forgets the request. */
 int qlb_server_result(qlb_server_t s, uint64_t request_id, double* expect_z, uint32_t num_qubits,

@@ -146,6 +146,7 @@ _PD = ctypes.POINTER(ctypes.c_double)
 _SIGNATURES = {
     "qlb_set_device": [_I],
     "qlb_device_info": [ctypes.POINTER(ctypes.c_int), _PU64, _PU64],
+    "qlb_selftest_bounded_wait": [_U32, ctypes.POINTER(ctypes.c_int)],
     "qlb_state_create": [ctypes.POINTER(_P)],
     "qlb_state_destroy": [_P],
     "qlb_state_initialize": [_P, _U32],
@@ -198,6 +199,7 @@ _SIGNATURES = {
     "qlb_server_wait": [_P, _U64, ctypes.c_double],
     "qlb_server_result": [_P, _U64, _P, _U32, _P, _U64, ctypes.POINTER(RequestInfo)],
     "qlb_server_stats": [_P, ctypes.POINTER(ServerInfo)],
+    "qlb_server_cancel": [_P, _U64],
     "qlb_server_destroy": [_P],
 }
 _OPTIONAL = {

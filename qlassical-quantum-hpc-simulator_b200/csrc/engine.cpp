@@ -378,6 +378,21 @@ int qlb_device_info(int* sm, uint64_t* free_b, uint64_t* total_b) {
     });
 }
 
+int qlb_selftest_bounded_wait(uint32_t limit_ms, int* gave_up) {
+    return guarded([&] {
+        need(gave_up, "gave_up");
+        if (limit_ms == 0 || limit_ms > 2000) fail(QLB_ERR_INVALID_ARG, "limit_ms must be in 1..2000");
+        DeviceBuffer flag;
+        int* d = static_cast<int*>(flag.ensure(256));
+        check_cuda(cudaMemset(d, 0, sizeof(int)), "flag clear");
+        check_cuda(launch_wait_selftest(uint64_t{limit_ms} * 1000000ull, d, nullptr), "wait self-test");
+        check_cuda(cudaStreamSynchronize(nullptr), "wait self-test sync");
+        int h = 0;
+        check_cuda(cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost), "flag D2H");
+        *gave_up = h;
+    });
+}
+
 // ---- state ---------------------------------------------------------------
 
 int qlb_state_create(qlb_state_t* out) {

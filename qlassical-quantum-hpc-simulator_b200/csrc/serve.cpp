@@ -86,7 +86,7 @@ private:
     std::map<size_t, size_t> free_;
 };
 
-enum ReqState { REQ_QUEUED = 0, REQ_ACTIVE = 1, REQ_DONE = 2, REQ_FAILED = 3 };
+enum ReqState { REQ_QUEUED = 0, REQ_ACTIVE = 1, REQ_DONE = 2, REQ_FAILED = 3, REQ_CANCELLED = 4 };
 
 struct Request {
     uint64_t id = 0;
@@ -99,6 +99,7 @@ struct Request {
     size_t o_state = 0, o_pass = 0, o_phase = 0, o_ops = 0, o_mat = 0, o_chunk = 0, o_samples = 0;
     std::vector<char> prog_image;   // passes | phases | ops | mats, offsets relative to o_pass
     uint32_t next_pass = 0;
+    bool cancel = false;            // set by qlb_server_cancel while admitted
     int status = REQ_QUEUED;
     std::string error;
     double t_submit = 0, t_admit = 0, t_done = 0;
@@ -320,10 +321,21 @@ void serve_loop(qlb_server* sp, int lane) {
             s.info.completed += 1;
         }
         for (auto& r : batch) r->next_pass += 1;
+        // cancelled requests leave at the round boundary: their kernels are done
+        bool dropped = false;
+        for (auto& r : L.active)
+            if (r->cancel && r->status == REQ_ACTIVE) {
+                r->status = REQ_CANCELLED;
+                r->t_done = s.now();
+                s.arena.release(r->block_off, r->block_bytes);
+                dropped = true;
+            }
         L.active.erase(std::remove_if(L.active.begin(), L.active.end(),
-                                      [](const std::shared_ptr<Request>& r) { return r->status == REQ_DONE; }),
+                                      [](const std::shared_ptr<Request>& r) {
+                                          return r->status == REQ_DONE || r->status == REQ_CANCELLED;
+                                      }),
                        L.active.end());
-        if (!finishing.empty()) {
+        if (!finishing.empty() || dropped) {
             s.cv_done.notify_all();
             s.cv_work.notify_all();   // freed arena blocks: the other lane may admit
         }
@@ -445,12 +457,32 @@ int qlb_server_wait(qlb_server_t s, uint64_t id, double timeout_s) {
         std::unique_lock<std::mutex> lk(s->mu);
         auto r = find(*s, id);
         const auto until = std::chrono::steady_clock::now() + std::chrono::duration<double>(timeout_s);
-        while (r->status != REQ_DONE && r->status != REQ_FAILED) {
-            if (s->cv_done.wait_until(lk, until) == std::cv_status::timeout &&
-                r->status != REQ_DONE && r->status != REQ_FAILED)
+        auto settled = [&] {
+            return r->status == REQ_DONE || r->status == REQ_FAILED || r->status == REQ_CANCELLED;
+        };
+        while (!settled()) {
+            if (s->cv_done.wait_until(lk, until) == std::cv_status::timeout && !settled())
                 fail(QLB_ERR_TIMEOUT, "request not finished within the timeout");
         }
         if (r->status == REQ_FAILED) fail(QLB_ERR_CUDA, r->error);
+        if (r->status == REQ_CANCELLED) fail(QLB_ERR_STATE, "request was cancelled");
+    });
+}
+
+int qlb_server_cancel(qlb_server_t s, uint64_t id) {
+    return guarded([&] {
+        need(s, "server");
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto r = find(*s, id);
+        if (r->status == REQ_QUEUED) {
+            for (Lane& L : s->lanes)
+                L.queue.erase(std::remove(L.queue.begin(), L.queue.end(), r), L.queue.end());
+            r->status = REQ_CANCELLED;
+            r->t_done = s->now();
+            s->cv_done.notify_all();
+        } else if (r->status == REQ_ACTIVE) {
+            r->cancel = true;   // leaves at the next round boundary
+        }
     });
 }
 
@@ -461,6 +493,10 @@ int qlb_server_result(qlb_server_t s, uint64_t id, double* expect_z, uint32_t nu
         std::lock_guard<std::mutex> lk(s->mu);
         auto r = find(*s, id);
         if (r->status == REQ_FAILED) fail(QLB_ERR_CUDA, r->error);
+        if (r->status == REQ_CANCELLED) {
+            s->all.erase(id);
+            fail(QLB_ERR_STATE, "request was cancelled");
+        }
         if (r->status != REQ_DONE) fail(QLB_ERR_STATE, "request not finished");
         if (expect_z) {
             if (num_qubits != r->n) fail(QLB_ERR_INVALID_ARG, "expect_z length must equal the request's qubits");

@@ -59,12 +59,13 @@ __device__ __forceinline__ uint64_t global_ns() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// Gives up after kWaitLimit polls or 2 s, whichever comes first.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+// Gives up after kWaitLimit polls or `limit_ns` (2 s), whichever comes first.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
+                                                  uint64_t limit_ns = 2000000000ull) {
     const uint64_t t0 = global_ns();
     for (uint32_t i = 0; i < kWaitLimit; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((i & 1023u) == 1023u && global_ns() - t0 > 2000000000ull) break;
+        if ((i & 1023u) == 1023u && global_ns() - t0 > limit_ns) break;
     }
     return false;
 }
@@ -792,7 +793,26 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
     }
 }
 
+// The tile kernel's bounded wait on an mbarrier that nothing completes: it
+// must give up after `limit_ns` and report through `err`, leaving the
+// context usable.
+__global__ void k_wait_selftest(uint64_t limit_ns, int* __restrict__ err) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar, 0u, limit_ns);
+    if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicExch(err, 1);
+}
+
 }  // namespace
+
+cudaError_t launch_wait_selftest(uint64_t limit_ns, int* err, cudaStream_t s) {
+    k_wait_selftest<<<1, 32, 0, s>>>(limit_ns, err);
+    return cudaGetLastError();
+}
 
 cudaError_t configure_tile_kernel() {
     static bool configured = false;

@@ -149,6 +149,10 @@ cudaError_t launch_tile_pass(float2* state, uint32_t n, const TilePass* d_passes
                              int* err, cudaStream_t s);
 int sm_count();   // multiprocessors of the current device (cached)
 
+// Runs the tile kernel's bounded mbarrier wait on a barrier that never
+// completes; *err becomes 1 when the wait gives up (as it must).
+cudaError_t launch_wait_selftest(uint64_t limit_ns, int* err, cudaStream_t s);
+
 // Sets the tile kernel's shared-memory limit (once per process; call before
 // capturing a launch into a CUDA graph).
 cudaError_t configure_tile_kernel();

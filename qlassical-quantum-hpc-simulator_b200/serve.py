@@ -59,6 +59,11 @@ class Server:
     def wait(self, rid: int, timeout: float = 600.0) -> None:
         call("qlb_server_wait", self._h, int(rid), float(timeout))
 
+    def cancel(self, rid: int) -> None:
+        """A queued request leaves at once, an admitted one at the next round
+        boundary; wait() / result() then raise RuntimeError."""
+        call("qlb_server_cancel", self._h, int(rid))
+
     def result(self, rid: int, timeout: float = 600.0) -> Result:
         self.wait(rid, timeout)
         n, shots = self._meta.pop(rid)

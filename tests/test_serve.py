@@ -77,3 +77,37 @@ def test_serve_admission_and_edge_cases():
         qc.measure(0)
         with pytest.raises(ValueError):
             srv.submit(qc.release())
+
+
+@pytest.mark.gpu
+def test_serve_cancel_queued_and_admitted():
+    """Host-side fault handling: cancelled requests leave the queue or the
+    running rounds, release their device memory, and do not disturb the
+    requests that share the server."""
+    import time
+    from qlassical_b200.serve import Server
+    with Server(memory_bytes=2 << 20) as srv:       # room for one 17-qubit request (1 MiB state)
+        a = circuits.random_h_rx_cx(17, 30, seed=1)
+        b = circuits.random_h_rx_cx(17, 30, seed=2)
+        ia = srv.submit(a, shots=0)
+        ib = srv.submit(b, shots=0)                  # waits for a's memory
+        srv.cancel(ib)
+        with pytest.raises(RuntimeError):
+            srv.result(ib)
+        got = srv.result(ia).expect_z
+        st, _ = oracle.run_oracle(a)
+        assert np.max(np.abs(got - circuits.expect_z_of(st, 17))) < 2e-5
+    with Server(memory_bytes=12 << 30) as srv:
+        big = srv.submit(circuits.random_h_rx_cx(30, 40, seed=3), shots=0)   # ~1 s of rounds
+        time.sleep(0.1)
+        assert srv.stats()["active"] == 1
+        srv.cancel(big)                              # admitted: leaves at the next round boundary
+        with pytest.raises(RuntimeError):
+            srv.result(big)
+        deadline = time.time() + 5.0
+        while srv.stats()["arena_used"] != 0 and time.time() < deadline:
+            time.sleep(0.01)
+        assert srv.stats()["arena_used"] == 0
+        c = circuits.random_h_rx_cx(14, 5, seed=4)
+        st, _ = oracle.run_oracle(c)
+        assert np.max(np.abs(srv.result(srv.submit(c, shots=0)).expect_z - circuits.expect_z_of(st, 14))) < 2e-5
