@@ -2,11 +2,17 @@
 
 Workload (one GPU): the 30-qubit complex64 (8.6 GB) random circuit of depth
 24 -- per layer RX/RY/RZ(theta~U[0,2pi)) on every qubit plus CZ on seeded
-random disjoint pairs (1080 gates) -- run through the tiled engine.  A step =
-one execution of the compiled circuit on a state already resident in HBM
-(reset to |0...0> between steps, untimed, like the reference benchmark loop,
-bench_hw_awareness.cpp:102-107).  amp-updates = gates x 2^n (pre-fusion
-gates, so fusion and tiling count as speed).
+random disjoint pairs (1080 gates) -- after the GPU middle end (fusion into
+dense blocks of up to 5 qubits plus qubit windowing, untimed as in the
+reference's benchmark), run with the 5-qubit blocks on the tensor cores.  A
+step = one execution of the compiled program on a state already resident in
+HBM (reset to |0...0> between steps, untimed, like the reference benchmark
+loop, bench_hw_awareness.cpp:102-107).  amp-updates = gates x 2^n
+(pre-fusion gates, so fusion and tiling count as speed).  The line also
+carries the same blocks on FP32 CUDA cores, the unfused circuit on the FP32
+tile path, one sweep per instruction, and a sampled-amplitude comparison of
+the tensor-core result with the unfused FP32 result.
+  python bench.py --circuit rot_cz | qft               the unfused circuit / the QFT (tiled)
 
   python bench.py [--gpus N --steps K --warmup W]      our engine (N replicas)
   python bench.py --impl reference                     the reference CPU engine
@@ -52,12 +58,14 @@ def parse():
     ap.add_argument("--qubits", type=int, default=30)
     ap.add_argument("--depth", type=int, default=24)
     ap.add_argument("--seed", type=int, default=1234)
-    ap.add_argument("--mode", default="tiled")
+    ap.add_argument("--mode", default=None,
+                    help="plain | tiled | tiled_tc (default: tiled_tc for the fused circuit, tiled otherwise)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--workload", default="circuit", choices=["circuit", "batched", "serving"])
-    ap.add_argument("--circuit", default="rot_cz", choices=["rot_cz", "qft", "fused"],
-                    help="circuit workload: random rotations + CZ (default), the same after k=5 fusion, or the QFT")
+    ap.add_argument("--circuit", default="fused", choices=["fused", "rot_cz", "qft"],
+                    help="circuit workload: the rotation + CZ circuit after k<=5 fusion and windowing (default), "
+                         "the same unfused, or the QFT")
     ap.add_argument("--circuits", type=int, default=4096, help="batched: circuits per batch")
     ap.add_argument("--requests", type=int, default=200, help="serving: requests")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: Poisson arrival rate (1/s)")
@@ -196,7 +204,10 @@ def run_reference(args):
     os.environ.setdefault("OMP_PLACES", "cores")
     from __graft_entry__ import package
     package()   # the circuit generators and IR types (no GPU work on this arm)
-    module = workload(args)
+    # The reference engine applies blocks of at most 4 qubits
+    # (cpu_openmp_engine.hpp:539-606): it gets the unfused circuit and fuses
+    # it with its own middle end.
+    module = workload(args) if args.circuit != "fused" else circuits_rot_cz(args)
     from oracle import oracle
     if not oracle.reference_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference sources absent)"}))
@@ -228,6 +239,7 @@ def run_ours(args):
     import torch.distributed as dist
     from __graft_entry__ import package
     q = package()
+    args.mode = args.mode or ("tiled_tc" if args.circuit == "fused" else "tiled")
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -314,23 +326,49 @@ def run_ours(args):
     extra = {"mode": args.mode, "passes_per_step": passes, "launches_per_step": pstats["launches"],
              "parallelism": f"replicas x{world}"}
     plain = None
+    comparisons = {}
+    check = None
     if not args.no_plain and rank == 0:
-        eng.reset()
-        eng.set_mode("plain")
-        pplan = eng.compile(module)
-        eng.reset()
-        eng.synchronize()
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record(stream)
-        eng.run(pplan)
-        e.record(stream)
-        eng.synchronize()
-        pms = s.elapsed_time(e)
-        pst = pplan.stats()
+        def one_run(mod, mode):
+            eng.set_mode(mode)
+            p = eng.compile(mod)
+            eng.reset()
+            eng.run(p)          # warm
+            eng.reset()
+            eng.synchronize()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            eng.run(p)
+            e.record(stream)
+            eng.synchronize()
+            st_ = p.stats()
+            del p
+            return s.elapsed_time(e), st_
+
+        pms, pst = one_run(module, "plain")
         plain = {"value": amp_updates_step / (pms / 1e3), "ms": pms, "sweeps": pst["sweeps"],
-                 "hbm_gbs": pst["sweeps"] * bytes_per_launch / (pms / 1e3) / 1e9}
+                 "kind": "one sweep per instruction (same circuit)"}
+        if args.circuit == "fused":
+            # the same fused blocks on FP32 CUDA cores, then the unfused circuit
+            # through the CUDA-core tile path; the last state is the reference
+            # for a sampled accuracy check of the tensor-core result
+            fms, _ = one_run(module, "tiled")
+            comparisons["fp32_fused"] = {"value": amp_updates_step / (fms / 1e3), "ms": fms}
+            rng = np.random.default_rng(5)
+            idx = rng.integers(0, 1 << n, size=1 << 16, dtype=np.uint64)
+            eng.set_mode(args.mode)
+            eng.reset()
+            eng.run(plan)
+            a_tc = eng.amplitudes_at(idx)
+            ums, _ = one_run(circuits_rot_cz(args), "tiled")
+            a_ref = eng.amplitudes_at(idx)
+            comparisons["unfused_fp32_tiles"] = {"value": amp_updates_step / (ums / 1e3), "ms": ums}
+            ip = np.vdot(a_ref, a_tc)
+            check = {"vs": "unfused circuit on the FP32 CUDA-core tile path", "sampled_amplitudes": int(idx.size),
+                     "max_abs_diff": float(np.max(np.abs(a_tc - a_ref))),
+                     "sampled_infidelity": float(1.0 - abs(ip) ** 2 / (np.vdot(a_ref, a_ref).real *
+                                                                       np.vdot(a_tc, a_tc).real))}
         eng.set_mode(args.mode)
-        del pplan
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -348,6 +386,10 @@ def run_ours(args):
     }
     if plain:
         line["plain_gpu"] = plain
+    if comparisons:
+        line["comparisons"] = comparisons
+    if check:
+        line["accuracy_check"] = check
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             # the reference engine takes blocks of <= 4 qubits: it runs the unfused circuit
