@@ -26,10 +26,13 @@ constexpr int NT = kTileThreads;            // 256
 constexpr int NR = 1 << kRegQubits;         // 32
 constexpr int TILE = 1 << kTileQubits;      // 8192
 constexpr uint32_t kWaitLimit = 1u << 26;
+// Tiles whose contiguous runs are at least 2^9 amplitudes (4 KB) go back to
+// HBM by bulk stores from shared memory; shorter runs by register stores.
+constexpr uint32_t kBulkStoreMinLow = 9;
 constexpr size_t kSmemBuffers = 3 * TILE * sizeof(float2);   // 2 TMA buffers + 1 transpose buffer
 constexpr size_t kSmemOps = kMaxSmemOps * sizeof(TileOp);
 constexpr size_t kSmemPhases = kMaxSmemPhases * sizeof(TilePhase);
-constexpr size_t kSmemMisc = 64;             // 2 TMA mbarriers, MMA and B-copy mbarriers, TMEM address
+constexpr size_t kSmemMisc = 64;             // 2 TMA mbarriers, the MMA mbarrier, TMEM address
 constexpr size_t kSmemTcB = 16384;           // B operand staging of a tensor-core op
 constexpr size_t kSmemTotal = kSmemBuffers + kSmemOps + kSmemPhases + sizeof(TilePass) + kSmemMisc + kSmemTcB;
 
@@ -76,6 +79,15 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
         "l"(src), "r"(bytes), "r"(smem_u32(bar))
         : "memory");
 }
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// This thread's bulk stores have finished reading shared memory / are complete.
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
@@ -106,6 +118,22 @@ __device__ __forceinline__ void issue_tile_load(float2* dst, const float2* __res
             if ((c >> (j - nl)) & 1u) g |= uint64_t{1} << P.tile_pos[j];
         bulk_g2s(dst + (static_cast<size_t>(c) << nl), state + g, bytes, bar);
     }
+}
+// The inverse: the tile, staged in `src` in the same linear layout, goes back
+// to HBM by bulk stores (one group per issuing thread).
+__device__ __forceinline__ void issue_tile_store(const float2* src, float2* __restrict__ state, const TilePass& P,
+                                                 uint64_t tile) {
+    const uint64_t base = tile_base(P, tile);
+    const uint32_t nl = P.n_low;
+    const uint32_t chunks = 1u << (kTileQubits - nl);
+    const uint32_t bytes = (1u << nl) * static_cast<uint32_t>(sizeof(float2));
+    for (uint32_t c = threadIdx.x; c < chunks; c += NT) {
+        uint64_t g = base;
+        for (uint32_t j = nl; j < static_cast<uint32_t>(kTileQubits); ++j)
+            if ((c >> (j - nl)) & 1u) g |= uint64_t{1} << P.tile_pos[j];
+        bulk_s2g(state + g, src + (static_cast<size_t>(c) << nl), bytes);
+    }
+    bulk_commit();
 }
 
 struct PhaseMap {
@@ -362,28 +390,40 @@ __device__ __forceinline__ void tc_ld_row(uint32_t taddr, uint32_t (&r)[64]) {
 struct TcCtx {
     uint32_t tmem;        // TMEM base address (lane 0, column base)
     uint64_t* bar;        // MMA-completion mbarrier
-    uint64_t* bbar;       // B-operand copy mbarrier
     unsigned char* sb;    // 16 KB B staging area
-    uint32_t uses;        // completed TC ops of this CTA (parity of both mbarriers)
+    uint32_t uses;        // completed TC ops of this CTA (parity of the mbarrier)
 };
+
+// B (16 KB, L2-resident: every tile of the pass reads the same image) is
+// fetched by all threads with cp.async through the load/store path.  A TMA
+// bulk copy would queue behind the 64 KB prefetch of the next tile in the
+// SM's copy engine and expose that tile's HBM latency inside the op.
+__device__ __forceinline__ void tc_fetch_b(unsigned char* sb, const float2* __restrict__ bimg) {
+    const unsigned char* src = reinterpret_cast<const unsigned char*>(bimg);
+#pragma unroll
+    for (uint32_t i = 0; i < kTcBBytes / (16u * NT); ++i) {
+        const uint32_t off = (i * NT + threadIdx.x) * 16u;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sb + off)), "l"(src + off)
+                     : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fetch_b_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // Applies one TC op; returns false if the MMA wait gave up (all threads agree).
 __device__ __forceinline__ bool op_dense_tc(float2 (&v)[NR], const float2* __restrict__ bimg, float2* cur,
                                             TcCtx& tc) {
     unsigned char* a_hi = reinterpret_cast<unsigned char*>(cur);
     unsigned char* a_lo = a_hi + 32768;
-    // B (16 KB) arrives by a bulk async copy while the CTA converts A; the
-    // staging area is free: the previous TC op's MMAs have completed.
-    if (threadIdx.x == 0) {
-        mbar_arrive_expect_tx(tc.bbar, kTcBBytes);
-        bulk_g2s(tc.sb, bimg, kTcBBytes, tc.bbar);
-    }
+    // B arrives while the CTA converts A; the staging area is free: the
+    // previous TC op's MMAs have completed.
+    tc_fetch_b(tc.sb, bimg);
     __syncthreads();          // everyone has read `cur`, which now receives A
     tc_write_a(v, a_hi, a_lo);
-    fence_proxy_async();      // generic writes of A -> visible to the tensor core
+    tc_fetch_b_wait();
+    fence_proxy_async();      // generic writes of A and B -> visible to the tensor core
     tc_fence_before();
-    const bool okb = mbar_wait_bounded(tc.bbar, tc.uses & 1u);
-    if (__syncthreads_or(!okb)) return false;
+    __syncthreads();
     if (threadIdx.x == 0) {
         tc_fence_after();
         const uint32_t ahi = smem_u32(a_hi), alo = smem_u32(a_lo), bhi = smem_u32(tc.sb), blo = bhi + 8192u;
@@ -656,7 +696,6 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
         mbar_init(&bar[2], 1);
-        mbar_init(&bar[3], 1);
         fence_mbar_init();
     }
     if (has_tc && threadIdx.x < 32) {     // warp 0 owns the tensor-memory allocation
@@ -668,7 +707,7 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    TcCtx tc{has_tc ? *tmem_holder : 0u, &bar[2], &bar[3], sb, 0u};
+    TcCtx tc{has_tc ? *tmem_holder : 0u, &bar[2], sb, 0u};
     bool failed = false;
 
     auto entry = [&](uint64_t t) -> TileWork { return n_work ? work[find_work(work, n_work, t)] : single; };
@@ -707,12 +746,30 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
         staged_prog = w.passes;
     };
 
+    // Pipeline: tile `it` lives in bufs[it & 1] (mbarrier bar[it & 1]).  The
+    // load of tile it + 2 is issued as soon as tile it has finished computing
+    // (its buffer is then free), so two loads are in flight while a tile is
+    // stored and the next one computes.  A finished tile of long runs is
+    // staged in the transpose buffer and written back by bulk stores, which
+    // drain while the CTA goes on; the next write into that buffer first
+    // waits until the stores have read it.
     uint64_t tile = blockIdx.x;
     float2* xbuf = bufs + 2 * static_cast<size_t>(TILE);
-    if (tile < ntiles) {
-        const TileWork w = entry(tile);
-        issue_tile_load(bufs, w.state, w.passes[w.pass], tile - w.tile_begin, &bar[0]);
-    }
+    auto issue_load = [&](uint64_t t, uint32_t slot) {
+        const TileWork wl = entry(t);
+        issue_tile_load(bufs + static_cast<size_t>(slot) * TILE, wl.state, wl.passes[wl.pass], t - wl.tile_begin,
+                        &bar[slot]);
+    };
+    if (tile < ntiles) issue_load(tile, 0);
+    if (tile + gridDim.x < ntiles) issue_load(tile + gridDim.x, 1);
+    bool store_pending = false;      // uniform: a bulk store may still be reading xbuf
+    auto xbuf_free = [&]() {
+        if (store_pending) {
+            bulk_wait_read();
+            __syncthreads();
+            store_pending = false;
+        }
+    };
     uint32_t it = 0;
     for (; tile < ntiles; tile += gridDim.x, ++it) {
         const TileWork w = entry(tile);
@@ -724,13 +781,7 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
         const TilePass& P = *spass;
         const uint32_t b = it & 1u;
         float2* cur = bufs + static_cast<size_t>(b) * TILE;
-        float2* nxt = bufs + static_cast<size_t>(b ^ 1u) * TILE;
         const uint64_t next = tile + gridDim.x;
-        if (next < ntiles) {
-            const TileWork wn = entry(next);
-            fence_proxy_async();   // earlier generic-proxy reads of nxt precede the async-proxy writes
-            issue_tile_load(nxt, wn.state, wn.passes[wn.pass], next - wn.tile_begin, &bar[b ^ 1u]);
-        }
         const bool ok = mbar_wait_bounded(&bar[b], (it >> 1) & 1u);
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) atomicExch(err, 1);
@@ -751,6 +802,7 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
         float2* rbuf = cur;
         for (uint32_t p = 1; p < nph && good; ++p) {
             float2* wbuf = (rbuf == xbuf) ? cur : xbuf;
+            if (wbuf == xbuf) xbuf_free();
 #pragma unroll
             for (int m = 0; m < NR; ++m) wbuf[slot_of(M, m)] = v[m];
             __syncthreads();
@@ -766,25 +818,39 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
             failed = true;
             break;
         }
-        // store: memory index of (thread, m) = gt | memory bits of m's register bits
-        const TilePhase& last = phases[nph - 1];
-        uint64_t ge[kRegQubits];
+        if (P.n_low >= kBulkStoreMinLow) {
+            // Stage the tile in xbuf (linear layout, as loaded); then cur is free.
+            if (store_pending) bulk_wait_read();
+            __syncthreads();             // every thread is done with cur and xbuf
 #pragma unroll
-        for (int j = 0; j < kRegQubits; ++j) ge[j] = uint64_t{1} << P.tile_pos[last.reg_pos[j]];
+            for (int m = 0; m < NR; ++m) xbuf[local_of(M, m)] = v[m];
+            fence_proxy_async();         // generic accesses of xbuf and cur precede the bulk copies
+            __syncthreads();
+            issue_tile_store(xbuf, state, P, tile - w.tile_begin);
+            store_pending = true;
+            if (next + gridDim.x < ntiles) issue_load(next + gridDim.x, b);
+        } else {
+            // Short runs: store from registers (the last phase's lanes are
+            // memory qubits 0..4, so a warp writes 256 contiguous bytes).
+            __syncthreads();             // every thread is done with cur
+            fence_proxy_async();         // ... before the async-proxy writes of the next load
+            if (next + gridDim.x < ntiles) issue_load(next + gridDim.x, b);
+            const TilePhase& last = phases[nph - 1];
+            uint64_t ge[kRegQubits];
 #pragma unroll
-        for (int m = 0; m < NR; ++m) {
-            uint64_t g = M.gt;
+            for (int j = 0; j < kRegQubits; ++j) ge[j] = uint64_t{1} << P.tile_pos[last.reg_pos[j]];
 #pragma unroll
-            for (int j = 0; j < kRegQubits; ++j)
-                if ((m >> j) & 1) g |= ge[j];
-            state[g] = v[m];
+            for (int m = 0; m < NR; ++m) {
+                uint64_t g = M.gt;
+#pragma unroll
+                for (int j = 0; j < kRegQubits; ++j)
+                    if ((m >> j) & 1) g |= ge[j];
+                state[g] = v[m];
+            }
         }
-        __syncthreads();   // everyone is done with `cur` before it is refilled
     }
-    if (failed && has_tc) {   // a late MMA or B copy, if any
-        mbar_wait_bounded(&bar[2], tc.uses & 1u);
-        mbar_wait_bounded(&bar[3], tc.uses & 1u);
-    }
+    bulk_wait_all();                     // this thread's bulk stores are complete
+    if (failed && has_tc) mbar_wait_bounded(&bar[2], tc.uses & 1u);   // a late MMA, if any
     tc_fence_before();
     __syncthreads();
     if (has_tc && threadIdx.x < 32) {
