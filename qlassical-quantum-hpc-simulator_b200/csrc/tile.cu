@@ -26,13 +26,14 @@ constexpr int NT = kTileThreads;            // 256
 constexpr int NR = 1 << kRegQubits;         // 32
 constexpr int TILE = 1 << kTileQubits;      // 8192
 constexpr uint32_t kWaitLimit = 1u << 26;
-// Tiles whose contiguous runs are at least 2^9 amplitudes (4 KB) go back to
-// HBM by bulk stores from shared memory; shorter runs by register stores.
-constexpr uint32_t kBulkStoreMinLow = 9;
+// Tiles whose contiguous runs are at least 2^9 amplitudes (4 KB) move by TMA
+// bulk copies (at most 16 per tile) in both directions; shorter runs load by
+// cp.async and store from registers.
+constexpr uint32_t kBulkMinLow = 9;
 constexpr size_t kSmemBuffers = 3 * TILE * sizeof(float2);   // 2 TMA buffers + 1 transpose buffer
 constexpr size_t kSmemOps = kMaxSmemOps * sizeof(TileOp);
 constexpr size_t kSmemPhases = kMaxSmemPhases * sizeof(TilePhase);
-constexpr size_t kSmemMisc = 64;             // 2 TMA mbarriers, the MMA mbarrier, TMEM address
+constexpr size_t kSmemMisc = 64;             // 2 tile mbarriers, the MMA mbarrier, TMEM address
 constexpr size_t kSmemTcB = 16384;           // B operand staging of a tensor-core op
 constexpr size_t kSmemTotal = kSmemBuffers + kSmemOps + kSmemPhases + sizeof(TilePass) + kSmemMisc + kSmemTcB;
 
@@ -45,6 +46,9 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
@@ -100,24 +104,50 @@ __device__ __forceinline__ uint64_t tile_base(const TilePass& P, uint64_t tile) 
     return base;
 }
 
-// All threads issue the TMA bulk copies of one tile into `dst` (one run of
-// 2^n_low amplitudes each); thread 0 registers the expected byte count.  The
-// mbarrier's transaction count may dip below zero when a copy completes
-// before the expectation is registered; the phase still completes only
-// after thread 0's arrival.
+// Loads one tile into `dst` (linear tile-local layout).  The tile mbarrier
+// expects one arrival per thread.  Runs of at least 2^kBulkMinLow amplitudes
+// go by TMA bulk copies (one per run, issued by all threads; thread 0 also
+// registers the byte count, and the transaction count may dip below zero
+// when a copy lands before that, but the phase cannot complete before
+// thread 0 arrives).  Shorter runs would need up to 256 bulk copies, which the
+// copy engine processes one after another, so they go by 16-byte cp.async
+// copies (16 per thread) whose completion each thread's deferred arrival
+// reports.
 __device__ __forceinline__ void issue_tile_load(float2* dst, const float2* __restrict__ state, const TilePass& P,
                                                 uint64_t tile, uint64_t* bar) {
-    if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, TILE * sizeof(float2));
     const uint64_t base = tile_base(P, tile);
     const uint32_t nl = P.n_low;
-    const uint32_t chunks = 1u << (kTileQubits - nl);
-    const uint32_t bytes = (1u << nl) * static_cast<uint32_t>(sizeof(float2));
-    for (uint32_t c = threadIdx.x; c < chunks; c += NT) {
-        uint64_t g = base;
-        for (uint32_t j = nl; j < static_cast<uint32_t>(kTileQubits); ++j)
-            if ((c >> (j - nl)) & 1u) g |= uint64_t{1} << P.tile_pos[j];
-        bulk_g2s(dst + (static_cast<size_t>(c) << nl), state + g, bytes, bar);
+    if (nl >= kBulkMinLow) {
+        const uint32_t chunks = 1u << (kTileQubits - nl);
+        const uint32_t bytes = (1u << nl) * static_cast<uint32_t>(sizeof(float2));
+        if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, TILE * sizeof(float2));
+        for (uint32_t c = threadIdx.x; c < chunks; c += NT) {
+            uint64_t g = base;
+            for (uint32_t j = nl; j < static_cast<uint32_t>(kTileQubits); ++j)
+                if ((c >> (j - nl)) & 1u) g |= uint64_t{1} << P.tile_pos[j];
+            bulk_g2s(dst + (static_cast<size_t>(c) << nl), state + g, bytes, bar);
+        }
+        if (threadIdx.x != 0) mbar_arrive(bar);
+        return;
     }
+    // Piece i of this thread holds tile-local amplitudes l, l + 1 with
+    // l = 512 i + 2 t: bits 1..8 of l come from the thread, bits 9..12 from i
+    // (all >= n_low here, so through tile_pos; bits below n_low map to themselves).
+    auto mem_bit = [&](uint32_t j) -> uint64_t { return uint64_t{1} << (j < nl ? j : P.tile_pos[j]); };
+    uint64_t gt = base;
+    for (uint32_t j = 1; j <= 8; ++j)
+        if ((threadIdx.x >> (j - 1)) & 1u) gt |= mem_bit(j);
+    const uint64_t hb[4] = {mem_bit(9), mem_bit(10), mem_bit(11), mem_bit(12)};
+#pragma unroll
+    for (uint32_t i = 0; i < 16; ++i) {
+        uint64_t g = gt;
+#pragma unroll
+        for (uint32_t k = 0; k < 4; ++k)
+            if ((i >> k) & 1u) g |= hb[k];
+        const uint32_t l = 512u * i + 2u * threadIdx.x;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst + l)), "l"(state + g) : "memory");
+    }
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 // The inverse: the tile, staged in `src` in the same linear layout, goes back
 // to HBM by bulk stores (one group per issuing thread).
@@ -394,33 +424,26 @@ struct TcCtx {
     uint32_t uses;        // completed TC ops of this CTA (parity of the mbarrier)
 };
 
-// B (16 KB, L2-resident: every tile of the pass reads the same image) is
-// fetched by all threads with cp.async through the load/store path.  A TMA
-// bulk copy would queue behind the 64 KB prefetch of the next tile in the
-// SM's copy engine and expose that tile's HBM latency inside the op.
-__device__ __forceinline__ void tc_fetch_b(unsigned char* sb, const float2* __restrict__ bimg) {
-    const unsigned char* src = reinterpret_cast<const unsigned char*>(bimg);
-#pragma unroll
-    for (uint32_t i = 0; i < kTcBBytes / (16u * NT); ++i) {
-        const uint32_t off = (i * NT + threadIdx.x) * 16u;
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sb + off)), "l"(src + off)
-                     : "memory");
-    }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fetch_b_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
 // Applies one TC op; returns false if the MMA wait gave up (all threads agree).
+// B (16 KB, L2-resident: every tile of the pass reads the same image) is
+// loaded by all threads with plain loads whose latency hides behind the A
+// conversion.  Neither a bulk copy (it would queue behind the next tile's
+// bulk prefetch in the copy engine) nor cp.async (its wait would include the
+// next tile's cp.async prefetch) is independent of the tile pipeline.
 __device__ __forceinline__ bool op_dense_tc(float2 (&v)[NR], const float2* __restrict__ bimg, float2* cur,
                                             TcCtx& tc) {
     unsigned char* a_hi = reinterpret_cast<unsigned char*>(cur);
     unsigned char* a_lo = a_hi + 32768;
-    // B arrives while the CTA converts A; the staging area is free: the
-    // previous TC op's MMAs have completed.
-    tc_fetch_b(tc.sb, bimg);
+    const uint4* bsrc = reinterpret_cast<const uint4*>(bimg);
+    uint4 bq[kTcBBytes / (16u * NT)];
+#pragma unroll
+    for (uint32_t i = 0; i < kTcBBytes / (16u * NT); ++i) bq[i] = __ldg(bsrc + i * NT + threadIdx.x);
     __syncthreads();          // everyone has read `cur`, which now receives A
     tc_write_a(v, a_hi, a_lo);
-    tc_fetch_b_wait();
+    // the staging area is free: the previous TC op's MMAs have completed
+    uint4* bdst = reinterpret_cast<uint4*>(tc.sb);
+#pragma unroll
+    for (uint32_t i = 0; i < kTcBBytes / (16u * NT); ++i) bdst[i * NT + threadIdx.x] = bq[i];
     fence_proxy_async();      // generic writes of A and B -> visible to the tensor core
     tc_fence_before();
     __syncthreads();
@@ -693,8 +716,8 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
     unsigned char* sb = smem_raw + kSmemBuffers + kSmemOps + kSmemPhases + sizeof(TilePass) + kSmemMisc;
 
     if (threadIdx.x == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        mbar_init(&bar[0], NT);          // tile loads: one arrival per thread
+        mbar_init(&bar[1], NT);
         mbar_init(&bar[2], 1);
         fence_mbar_init();
     }
@@ -757,8 +780,11 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
     float2* xbuf = bufs + 2 * static_cast<size_t>(TILE);
     auto issue_load = [&](uint64_t t, uint32_t slot) {
         const TileWork wl = entry(t);
-        issue_tile_load(bufs + static_cast<size_t>(slot) * TILE, wl.state, wl.passes[wl.pass], t - wl.tile_begin,
-                        &bar[slot]);
+        // the staged shared-memory copy of the pass when it is the same pass
+        // (always, for a single state): its address bits are cheap to read
+        const bool same = wl.pass == staged && wl.passes == staged_prog;
+        issue_tile_load(bufs + static_cast<size_t>(slot) * TILE, wl.state, same ? *spass : wl.passes[wl.pass],
+                        t - wl.tile_begin, &bar[slot]);
     };
     if (tile < ntiles) issue_load(tile, 0);
     if (tile + gridDim.x < ntiles) issue_load(tile + gridDim.x, 1);
@@ -818,7 +844,7 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
             failed = true;
             break;
         }
-        if (P.n_low >= kBulkStoreMinLow) {
+        if (P.n_low >= kBulkMinLow) {
             // Stage the tile in xbuf (linear layout, as loaded); then cur is free.
             if (store_pending) bulk_wait_read();
             __syncthreads();             // every thread is done with cur and xbuf
