@@ -675,32 +675,42 @@ private:
         return f;
     }
 
-    // B operand image (hi 8 KB + lo 8 KB, K-major canonical layout) of the
-    // real embedding of the 32x32 unitary U (row-major, FP64).
-    void emit_tc_op(const std::vector<cd>& U) {
+    // B operand image (hi 8 KB + lo 8 KB, K-major canonical layout without
+    // swizzle) of the real embedding of the 32x32 unitary U (row-major,
+    // FP64): row n = 2 r + ro (output amplitude r, real / imaginary part),
+    // column k = 2 kappa(c) + ri (input amplitude c, real / imaginary part),
+    // kappa(c) placing bit j of c at bit kperm[j].  op.flags records kperm
+    // (3 bits per register bit).
+    void emit_tc_op(const std::vector<cd>& U, const int* kperm = nullptr) {
+        static const int ident[kRegQubits] = {0, 1, 2, 3, 4};
+        if (!kperm) kperm = ident;
         if (prog.mats.size() & 1) prog.mats.push_back(make_float2(0.f, 0.f));
         const uint32_t off = static_cast<uint32_t>(prog.mats.size());
         prog.mats.resize(prog.mats.size() + 2048, make_float2(0.f, 0.f));
         unsigned char* img = reinterpret_cast<unsigned char*>(prog.mats.data() + off);
-        for (int n = 0; n < 64; ++n)
-            for (int kk = 0; kk < 64; ++kk) {
-                const int r = n & 31, c = kk & 31;
-                const cd u = U[r * 32 + c];
-                double x;
-                if (n < 32) x = kk < 32 ? u.real() : -u.imag();
-                else x = kk < 32 ? u.imag() : u.real();
-                const uint16_t hi = bf16_rn(static_cast<float>(x));
-                const uint16_t lo = bf16_rn(static_cast<float>(x - static_cast<double>(bf16_f(hi))));
-                const size_t at = static_cast<size_t>(n / 8) * 1024 + static_cast<size_t>(kk / 8) * 128 +
-                                  static_cast<size_t>(n % 8) * 16 + static_cast<size_t>(kk % 8) * 2;
-                std::memcpy(img + at, &hi, 2);
-                std::memcpy(img + 8192 + at, &lo, 2);
-            }
+        for (int c = 0; c < 32; ++c) {
+            int kc = 0;
+            for (int j = 0; j < kRegQubits; ++j)
+                if ((c >> j) & 1) kc |= 1 << kperm[j];
+            for (int n = 0; n < 64; ++n)
+                for (int ri = 0; ri < 2; ++ri) {
+                    const int r = n >> 1, ro = n & 1, kk = 2 * kc + ri;
+                    const cd u = U[r * 32 + c];
+                    const double x = ro == 0 ? (ri == 0 ? u.real() : -u.imag()) : (ri == 0 ? u.imag() : u.real());
+                    const uint16_t hi = bf16_rn(static_cast<float>(x));
+                    const uint16_t lo = bf16_rn(static_cast<float>(x - static_cast<double>(bf16_f(hi))));
+                    const size_t at = static_cast<size_t>(n / 8) * 1024 + static_cast<size_t>(kk / 8) * 128 +
+                                      static_cast<size_t>(n % 8) * 16 + static_cast<size_t>(kk % 8) * 2;
+                    std::memcpy(img + at, &hi, 2);
+                    std::memcpy(img + 8192 + at, &lo, 2);
+                }
+        }
         TileOp op{};
         op.kind = TOP_DENSE_TC;
         op.code = OPC_DENSE_TC;
         op.k = 5;
         op.data = off;
+        for (int j = 0; j < kRegQubits; ++j) op.flags |= static_cast<uint32_t>(kperm[j]) << (3 * j);
         prog.ops.push_back(op);
         stats.dense_ops += 1;
         stats.tc_ops += 1;

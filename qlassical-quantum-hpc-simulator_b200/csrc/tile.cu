@@ -334,13 +334,18 @@ __device__ __forceinline__ void op_dense5(float2 (&v)[NR], const float2* __restr
 //
 // A 32x32 complex unitary U on the five register qubits, applied to all 256
 // register groups of the tile at once:  D = A * B^T with
-//   A[row t][k]  = x_t[k],   x_t = (Re a_0..Re a_31, Im a_0..Im a_31)  (thread t = row t)
-//   B[n][k]      = real embedding of U: [[Re U, -Im U], [Im U, Re U]]
-// in bf16 split precision: D = Ahi*Bhi + Ahi*Blo + Alo*Bhi, FP32 accumulate
-// in tensor memory (rows 0..127 -> TMEM columns 0..63, rows 128..255 ->
-// columns 64..127).  Both operands use the K-major, no-swizzle canonical
-// layout: 8 x 16 B core matrices, LBO = 128 B between the K chunks of one
-// row group, SBO = 1024 B between 8-row groups (K = 64 -> 8 chunks).
+//   A[row t][k]  = x_t[k],  k = 2 kappa(m) + ri:  Re / Im of amplitude m of thread t
+//                  (kappa: a permutation of the 5 register bits, fixed per op)
+//   B[n][k]      = real embedding of U, n = 2 r + ro:  B[2r][2c] = Re U_rc,
+//                  B[2r][2c+1] = -Im U_rc, B[2r+1][2c] = Im U_rc, B[2r+1][2c+1] = Re U_rc
+// (k, n interleave real and imaginary parts) in bf16 split precision:
+// D = Ahi*Bhi + Ahi*Blo + Alo*Bhi, FP32 accumulate in tensor memory (rows
+// 0..127 -> TMEM columns 0..63, rows 128..255 -> columns 64..127).
+// A is K-major with the 128-byte swizzle: row t at byte 128 t, its 16-byte
+// chunk j (k = 8j .. 8j+7) at chunk position j ^ (t & 7); 8-row groups 1024 B
+// apart (SBO).  B is K-major without swizzle: 8 x 16 B core matrices,
+// LBO = 128 B between the K chunks of one row group, SBO = 1024 B between
+// 8-row groups.  D column n of row t is read back by thread t.
 constexpr uint32_t kTcCols = 128;
 constexpr uint32_t kTcBBytes = 16384;          // B hi (8 KB) + B lo (8 KB)
 constexpr uint32_t kTcIdesc = (1u << 4)        // D format F32
@@ -349,36 +354,43 @@ constexpr uint32_t kTcIdesc = (1u << 4)        // D format F32
                               | ((64u >> 3) << 17)    // N = 64
                               | ((128u >> 4) << 24);  // M = 128
 
-__device__ __forceinline__ uint64_t umma_desc(uint32_t smem_addr) {
+// B: no swizzle, LBO 128 B, SBO 1024 B.
+__device__ __forceinline__ uint64_t umma_desc_b(uint32_t smem_addr) {
     return static_cast<uint64_t>((smem_addr >> 4) & 0x3FFFu) | (static_cast<uint64_t>(128u >> 4) << 16) |
            (static_cast<uint64_t>(1024u >> 4) << 32) | (uint64_t{1} << 46);
+}
+// A: 128-byte swizzle (layout code 2), SBO 1024 B (LBO unused: K fits one
+// swizzle row).  K steps advance the start address by 32 B inside the
+// 1024-byte-aligned swizzle atom.
+__device__ __forceinline__ uint64_t umma_desc_a(uint32_t smem_addr) {
+    return static_cast<uint64_t>((smem_addr >> 4) & 0x3FFFu) | (uint64_t{1} << 16) |
+           (static_cast<uint64_t>(1024u >> 4) << 32) | (uint64_t{1} << 46) | (uint64_t{2} << 61);
 }
 
 __device__ __forceinline__ float bf16_to_float(uint32_t b) { return __uint_as_float(b << 16); }
 
-// Writes this thread's row of A (hi and lo) into the canonical layout.
+// (re, im) -> hi = bf16x2(re, im), lo = bf16x2 of the residuals (re in the low half).
+__device__ __forceinline__ void tc_split(float2 x, uint32_t& hi, uint32_t& lo) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(x.x, x.y);
+    const uint32_t hb = *reinterpret_cast<const uint32_t*>(&h);
+    const float2 r = __fadd2_rn(x, make_float2(-bf16_to_float(hb & 0xFFFFu), -__uint_as_float(hb & 0xFFFF0000u)));
+    const __nv_bfloat162 l = __floats2bfloat162_rn(r.x, r.y);
+    hi = hb;
+    lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
+// Writes this thread's row of A (hi and lo), kappa = identity: chunk j holds
+// amplitudes 4j .. 4j+3.
 __device__ __forceinline__ void tc_write_a(const float2 (&v)[NR], unsigned char* a_hi, unsigned char* a_lo) {
     const uint32_t t = threadIdx.x;
-    const uint32_t rowoff = (t >> 3) * 1024u + (t & 7u) * 16u;
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {           // K chunk c = reals 8c .. 8c+7
+    for (uint32_t j = 0; j < 8; ++j) {
         uint32_t hi[4], lo[4];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            // two reals per instruction: x -> hi = bf16(x), lo = bf16(x - hi)
-            const int k0 = c * 8 + 2 * e;
-            const float x0 = k0 < 32 ? v[k0].x : v[k0 - 32].y;
-            const float x1 = (k0 + 1) < 32 ? v[k0 + 1].x : v[k0 + 1 - 32].y;
-            const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
-            const uint32_t hb = *reinterpret_cast<const uint32_t*>(&h);
-            const float2 r = __fadd2_rn(make_float2(x0, x1),
-                                        make_float2(-bf16_to_float(hb & 0xFFFFu), -__uint_as_float(hb & 0xFFFF0000u)));
-            const __nv_bfloat162 l = __floats2bfloat162_rn(r.x, r.y);
-            hi[e] = hb;
-            lo[e] = *reinterpret_cast<const uint32_t*>(&l);
-        }
-        *reinterpret_cast<uint4*>(a_hi + rowoff + c * 128u) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-        *reinterpret_cast<uint4*>(a_lo + rowoff + c * 128u) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+        for (int e = 0; e < 4; ++e) tc_split(v[4 * j + e], hi[e], lo[e]);
+        const uint32_t off = t * 128u + ((j ^ (t & 7u)) << 4);
+        *reinterpret_cast<uint4*>(a_hi + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+        *reinterpret_cast<uint4*>(a_lo + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
     }
 }
 
@@ -457,8 +469,8 @@ __device__ __forceinline__ bool op_dense_tc(float2 (&v)[NR], const float2* __res
             for (int p = 0; p < 3; ++p)
 #pragma unroll
                 for (uint32_t s = 0; s < 4; ++s)
-                    tc_mma(tc.tmem + mb * 64u, umma_desc(as[p] + mb * 16384u + s * 256u),
-                           umma_desc(bs[p] + s * 256u), (p > 0 || s > 0) ? 1u : 0u);
+                    tc_mma(tc.tmem + mb * 64u, umma_desc_a(as[p] + mb * 16384u + s * 32u),
+                           umma_desc_b(bs[p] + s * 256u), (p > 0 || s > 0) ? 1u : 0u);
         tc_commit(tc.bar);
     }
     const bool ok = mbar_wait_bounded(tc.bar, tc.uses & 1u);
@@ -469,7 +481,7 @@ __device__ __forceinline__ bool op_dense_tc(float2 (&v)[NR], const float2* __res
     uint32_t r[64];
     tc_ld_row(tc.tmem + (((w & 3u) * 32u) << 16) + (w >> 2) * 64u, r);
 #pragma unroll
-    for (int c = 0; c < NR; ++c) v[c] = make_float2(__uint_as_float(r[c]), __uint_as_float(r[32 + c]));
+    for (int c = 0; c < NR; ++c) v[c] = make_float2(__uint_as_float(r[2 * c]), __uint_as_float(r[2 * c + 1]));
     tc_fence_before();
     return true;
 }

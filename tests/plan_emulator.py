@@ -74,7 +74,7 @@ def emulate(plan, init=None):
                         D = 1 << k
                         apply_k(st, n, mq[:k], mats[op["data"]:op["data"] + D * D].reshape(D, D), cmask)
                     elif kd == TOP_DENSE_TC:
-                        apply_k(st, n, mq[:5], decode_tc_flat(plan, op["data"]), 0)
+                        apply_k(st, n, mq[:5], decode_tc_flat(plan, op["data"], op["flags"]), 0)
                     elif kd == TOP_DIAG:
                         apply_diag(st, n, mq, op, words, tq)
                     elif kd == TOP_CPHASE:
@@ -163,8 +163,11 @@ def apply_diag(st, n, mq, op, words, tq):
 _tc_cache = {}
 
 
-def decode_tc_flat(plan, data):
-    key = (id(plan), data)
+def decode_tc_flat(plan, data, flags=None):
+    """The split-precision unitary of a tensor-core op from its B image: row
+    n = 2r + ro, column k = 2 kappa(c) + ri, kappa placing bit j of c at bit
+    (flags >> 3j) & 7 (identity when flags is None)."""
+    key = (id(plan), data, flags)
     if key not in _tc_cache:
         flat = np.array(plan["mats"], dtype=np.uint32)    # raw words, 2 per float2 slot
         raw = flat[2 * data:2 * data + 4096].tobytes()
@@ -175,5 +178,7 @@ def decode_tc_flat(plan, data):
         hi = (u16[at // 2] << 16).astype(np.uint32).view(np.float32).astype(np.float64)
         lo = (u16[(8192 + at) // 2] << 16).astype(np.uint32).view(np.float32).astype(np.float64)
         B = hi + lo
-        _tc_cache[key] = B[:32, :32] + 1j * B[32:, :32]
+        perm = [j for j in range(5)] if flags is None else [(flags >> (3 * j)) & 7 for j in range(5)]
+        kap = np.array([sum(((c >> j) & 1) << perm[j] for j in range(5)) for c in range(32)])
+        _tc_cache[key] = B[0::2][:, 2 * kap] + 1j * B[1::2][:, 2 * kap]
     return _tc_cache[key]
