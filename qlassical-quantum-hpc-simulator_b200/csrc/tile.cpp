@@ -176,6 +176,114 @@ void choose_threads(const std::vector<int>& reg, bool edge, uint8_t* thr) {
     for (int j = 0; j < kThreadQubits; ++j) thr[j] = static_cast<uint8_t>(order[j]);
 }
 
+// ---- tensor-core phase entry ----------------------------------------------
+// The A operand of a tensor-core op (128-byte swizzle, real and imaginary
+// parts interleaved along K) puts the amplitude at tile-local index i at the
+// XOR over i's set bits p of a_offset(p): register bit j of the phase is K
+// bit kperm[j] (byte 4 << kperm[j]); thread bit j is row bit j (byte 128 << j,
+// and for j < 3 the swizzle flips chunk bit j, byte 16 << j).
+uint16_t a_offset(const TilePhase& ph, const int* kperm, int p) {
+    for (int j = 0; j < kRegQubits; ++j)
+        if (ph.reg_pos[j] == p) return static_cast<uint16_t>(4u << kperm[j]);
+    for (int j = 0; j < kThreadQubits; ++j)
+        if (ph.thr_pos[j] == p) return static_cast<uint16_t>((128u << j) ^ (j < 3 ? (16u << j) : 0u));
+    return 0;
+}
+
+// Rank over GF(2) of the shared-memory bank bits (word address bits 0..4) of
+// the previous phase's five lane positions: the 4-byte A stores of one warp
+// instruction hit 2^(5 - rank) times the same bank.
+int entry_bank_rank(const TilePhase& prev, const TilePhase& ph, const int* kperm) {
+    uint32_t rows[5];
+    for (int j = 0; j < 5; ++j) rows[j] = (a_offset(ph, kperm, prev.thr_pos[j]) >> 2) & 31u;
+    int rank = 0;
+    for (int bit = 4; bit >= 0; --bit) {
+        int piv = -1;
+        for (int j = rank; j < 5; ++j)
+            if ((rows[j] >> bit) & 1u) {
+                piv = j;
+                break;
+            }
+        if (piv < 0) continue;
+        std::swap(rows[rank], rows[piv]);
+        for (int j = 0; j < 5; ++j)
+            if (j != rank && ((rows[j] >> bit) & 1u)) rows[j] ^= rows[rank];
+        ++rank;
+    }
+    return rank;
+}
+
+// The K permutation (of 120) with the fewest bank conflicts for the entry
+// stores; the first found among equals, so the identity when it is as good.
+void choose_kperm(const TilePhase& prev, const TilePhase& ph, int* kperm) {
+    int p[kRegQubits] = {0, 1, 2, 3, 4};
+    int best = -1;
+    do {
+        const int r = entry_bank_rank(prev, ph, p);
+        if (r > best) {
+            best = r;
+            std::copy(p, p + kRegQubits, kperm);
+            if (r == 5) break;
+        }
+    } while (std::next_permutation(p, p + kRegQubits));
+}
+
+// Thread order of a phase entered from the previous phase's registers: the
+// previous lanes that become thread bits go to thread bits 0..2 (their rows
+// flip distinct swizzle bits), from the highest of those slots down, leaving
+// the low slots' banks to previous lanes that become register bits; the other
+// lane slots take qubits the next phase holds in registers (so that entry
+// has register-bound lanes too); then the rest in order.
+void choose_threads_entry(const std::vector<int>& reg, const uint8_t* prev_thr, const std::vector<int>* next_reg,
+                          uint8_t* thr) {
+    bool in_reg[kTileQubits] = {}, used[kTileQubits] = {};
+    for (int p : reg) in_reg[p] = true;
+    int slot[kThreadQubits];
+    std::fill(slot, slot + kThreadQubits, -1);
+    std::vector<int> to_thr;
+    int a = 0;
+    for (int j = 0; j < 5; ++j) {
+        if (in_reg[prev_thr[j]]) ++a;
+        else to_thr.push_back(prev_thr[j]);
+    }
+    // slots 2, 1, 0 (bank bits 4, 3, 2) for up to three of them, the others at 3, 4, ...
+    int s = 2, extra = 3;
+    for (int p : to_thr) {
+        int at;
+        if (s >= 0 && s >= a - 2) at = s--;
+        else at = extra++;
+        slot[at] = p;
+        used[p] = true;
+    }
+    std::vector<int> pref, rest;
+    if (next_reg)
+        for (int p : *next_reg)
+            if (!in_reg[p] && !used[p]) pref.push_back(p);
+    for (int p = 0; p < kTileQubits; ++p)
+        if (!in_reg[p] && !used[p] && std::find(pref.begin(), pref.end(), p) == pref.end()) rest.push_back(p);
+    std::vector<int> order = pref;
+    order.insert(order.end(), rest.begin(), rest.end());
+    // without a next entry to prepare, lanes 0..3 take distinct residues mod 4
+    // where they can (conflict-free transposes under the XOR fold)
+    bool res_used[4] = {};
+    for (int j = 0; j < 4; ++j)
+        if (slot[j] >= 0) res_used[slot[j] % 4] = true;
+    for (int j = 0; j < kThreadQubits; ++j) {
+        if (slot[j] >= 0) continue;
+        size_t pick = 0;
+        if (!next_reg && j < 4)
+            for (size_t i = 0; i < order.size(); ++i)
+                if (!res_used[order[i] % 4]) {
+                    pick = i;
+                    break;
+                }
+        slot[j] = order[pick];
+        if (j < 4) res_used[slot[j] % 4] = true;
+        order.erase(order.begin() + static_cast<long>(pick));
+    }
+    for (int j = 0; j < kThreadQubits; ++j) thr[j] = static_cast<uint8_t>(slot[j]);
+}
+
 void fill_reg(std::vector<int>& reg, bool edge) {
     bool in_reg[kTileQubits] = {};
     for (int p : reg) in_reg[p] = true;
@@ -408,17 +516,42 @@ private:
             if (low) phases.push_back(PhaseBuild{});  // store phase with lanes on qubits 0..4
         }
         P.phase_begin = static_cast<uint32_t>(prog.phases.size());
+        for (size_t pi = 0; pi < phases.size(); ++pi)
+            fill_reg(phases[pi].reg, (pi == 0) || (pi + 1 == phases.size()));
+        const bool tcm = e_.mode == QLB_MODE_TILED_TC;
         for (size_t pi = 0; pi < phases.size(); ++pi) {
             PhaseBuild& pb = phases[pi];
             const bool edge = (pi == 0) || (pi + 1 == phases.size());
-            fill_reg(pb.reg, edge);
             TilePhase ph{};
             for (int r = 0; r < kRegQubits; ++r) ph.reg_pos[r] = static_cast<uint8_t>(pb.reg[r]);
-            choose_threads(pb.reg, edge, ph.thr_pos);
+            // A phase that opens with a non-diagonal instruction in tensor-core
+            // mode will likely open with its tensor-core op: it may be entered
+            // straight from the previous phase's registers (kPhaseTcEntry).
+            const bool cand = tcm && pi > 0 && !pb.ops.empty() && !mi[pb.ops[0]].diag;
+            const TilePhase* prev = pi > 0 ? &prog.phases.back() : nullptr;
+            if (cand && !edge) {
+                // the next phase's registers, when it is itself an entry candidate
+                const bool next_cand = pi + 1 < phases.size() && !phases[pi + 1].ops.empty() &&
+                                       !mi[phases[pi + 1].ops[0]].diag;
+                const std::vector<int>* next_reg = next_cand ? &phases[pi + 1].reg : nullptr;
+                choose_threads_entry(pb.reg, prev->thr_pos, next_reg, ph.thr_pos);
+            } else {
+                choose_threads(pb.reg, edge, ph.thr_pos);
+            }
             for (int j = 0; j < kThreadQubits; ++j) pb.thr_mem[j] = bitm(P.tile_pos[ph.thr_pos[j]]);
             ph.op_begin = static_cast<uint32_t>(prog.ops.size());
+            if (cand) {
+                choose_kperm(*prev, ph, entry_kperm_);
+                entry_op_ = ph.op_begin;
+            }
             encode_ops(pb, P, local_of, final_pass && pi + 1 == phases.size());
+            entry_op_ = ~0u;
             ph.op_end = static_cast<uint32_t>(prog.ops.size());
+            if (cand && ph.op_end > ph.op_begin && prog.ops[ph.op_begin].kind == TOP_DENSE_TC) {
+                ph.flags |= kPhaseTcEntry;
+                for (int j = 0; j < kThreadQubits; ++j) ph.a_thr[j] = a_offset(ph, entry_kperm_, prev->thr_pos[j]);
+                for (int j = 0; j < kRegQubits; ++j) ph.a_reg[j] = a_offset(ph, entry_kperm_, prev->reg_pos[j]);
+            }
             prog.phases.push_back(ph);
         }
         P.phase_end = static_cast<uint32_t>(prog.phases.size());
@@ -459,6 +592,10 @@ private:
     // RZ and diagonal UNITARYs); applied once at the end of its last phase.
     double pass_global_ = 0.0;
     int pass_features_ = 0;   // kPass* bits of the pass being built
+    // A tensor-core op emitted as op entry_op_ opens a kPhaseTcEntry
+    // candidate phase and takes the K permutation entry_kperm_.
+    uint32_t entry_op_ = ~0u;
+    int entry_kperm_[kRegQubits] = {0, 1, 2, 3, 4};
 
     // ---- FP64 form of one register-level op --------------------------------
     using cd = std::complex<double>;
@@ -736,7 +873,7 @@ private:
                 for (const HostOp& h : acc.ops) apply_host(h, col);
                 for (int r = 0; r < 32; ++r) U[r * 32 + c] = col[r];
             }
-            emit_tc_op(U);
+            emit_tc_op(U, prog.ops.size() == entry_op_ ? entry_kperm_ : nullptr);
         }
         acc = Acc{};
     }
@@ -1204,6 +1341,18 @@ std::string describe_plan_json(const PlanConfig& cfg, const qlb_gate_instr* prog
             for (int j = 0; j < kThreadQubits; ++j) {
                 if (j) out += ",";
                 u(T.thr_pos[j]);
+            }
+            out += "],\"flags\":";
+            u(T.flags);
+            out += ",\"a_thr\":[";
+            for (int j = 0; j < kThreadQubits; ++j) {
+                if (j) out += ",";
+                u(T.a_thr[j]);
+            }
+            out += "],\"a_reg\":[";
+            for (int j = 0; j < kRegQubits; ++j) {
+                if (j) out += ",";
+                u(T.a_reg[j]);
             }
             out += "],\"ops\":[";
             for (uint32_t o = T.op_begin; o < T.op_end; ++o) {

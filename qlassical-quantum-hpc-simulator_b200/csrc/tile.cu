@@ -36,6 +36,8 @@ constexpr size_t kSmemPhases = kMaxSmemPhases * sizeof(TilePhase);
 constexpr size_t kSmemMisc = 64;             // 2 tile mbarriers, the MMA mbarrier, TMEM address
 constexpr size_t kSmemTcB = 16384;           // B operand staging of a tensor-core op
 constexpr size_t kSmemTotal = kSmemBuffers + kSmemOps + kSmemPhases + sizeof(TilePass) + kSmemMisc + kSmemTcB;
+static_assert((kSmemBuffers + kSmemOps + kSmemPhases + sizeof(TilePass)) % 16 == 0, "mbarriers and B staging alignment");
+static_assert(kSmemTotal <= 227 * 1024, "shared memory per CTA");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -436,32 +438,34 @@ struct TcCtx {
     uint32_t uses;        // completed TC ops of this CTA (parity of the mbarrier)
 };
 
-// Applies one TC op; returns false if the MMA wait gave up (all threads agree).
 // B (16 KB, L2-resident: every tile of the pass reads the same image) is
 // loaded by all threads with plain loads whose latency hides behind the A
 // conversion.  Neither a bulk copy (it would queue behind the next tile's
 // bulk prefetch in the copy engine) nor cp.async (its wait would include the
 // next tile's cp.async prefetch) is independent of the tile pipeline.
-__device__ __forceinline__ bool op_dense_tc(float2 (&v)[NR], const float2* __restrict__ bimg, float2* cur,
-                                            TcCtx& tc) {
-    unsigned char* a_hi = reinterpret_cast<unsigned char*>(cur);
-    unsigned char* a_lo = a_hi + 32768;
+constexpr uint32_t kTcBPerThread = kTcBBytes / (16u * NT);
+__device__ __forceinline__ void tc_load_b(const float2* __restrict__ bimg, uint4 (&bq)[kTcBPerThread]) {
     const uint4* bsrc = reinterpret_cast<const uint4*>(bimg);
-    uint4 bq[kTcBBytes / (16u * NT)];
 #pragma unroll
-    for (uint32_t i = 0; i < kTcBBytes / (16u * NT); ++i) bq[i] = __ldg(bsrc + i * NT + threadIdx.x);
-    __syncthreads();          // everyone has read `cur`, which now receives A
-    tc_write_a(v, a_hi, a_lo);
-    // the staging area is free: the previous TC op's MMAs have completed
+    for (uint32_t i = 0; i < kTcBPerThread; ++i) bq[i] = __ldg(bsrc + i * NT + threadIdx.x);
+}
+// Stores B (the staging area is free: the previous TC op's MMAs have
+// completed), makes A and B visible to the tensor core and synchronizes.
+__device__ __forceinline__ void tc_store_b_sync(const uint4 (&bq)[kTcBPerThread], TcCtx& tc) {
     uint4* bdst = reinterpret_cast<uint4*>(tc.sb);
 #pragma unroll
-    for (uint32_t i = 0; i < kTcBBytes / (16u * NT); ++i) bdst[i * NT + threadIdx.x] = bq[i];
+    for (uint32_t i = 0; i < kTcBPerThread; ++i) bdst[i * NT + threadIdx.x] = bq[i];
     fence_proxy_async();      // generic writes of A and B -> visible to the tensor core
     tc_fence_before();
     __syncthreads();
+}
+// Thread 0 issues the 24 MMAs of the op (A at a_hi, a_hi + 32 KB); everyone
+// waits for them and reads its row of D back into v (this phase's layout).
+// Returns false if the wait gave up (all threads agree).
+__device__ __forceinline__ bool tc_mma_readback(float2 (&v)[NR], const unsigned char* a_hi, TcCtx& tc) {
     if (threadIdx.x == 0) {
         tc_fence_after();
-        const uint32_t ahi = smem_u32(a_hi), alo = smem_u32(a_lo), bhi = smem_u32(tc.sb), blo = bhi + 8192u;
+        const uint32_t ahi = smem_u32(a_hi), alo = ahi + 32768u, bhi = smem_u32(tc.sb), blo = bhi + 8192u;
         const uint32_t as[3] = {ahi, ahi, alo}, bs[3] = {bhi, blo, bhi};
 #pragma unroll
         for (uint32_t mb = 0; mb < 2; ++mb)
@@ -484,6 +488,49 @@ __device__ __forceinline__ bool op_dense_tc(float2 (&v)[NR], const float2* __res
     for (int c = 0; c < NR; ++c) v[c] = make_float2(__uint_as_float(r[2 * c]), __uint_as_float(r[2 * c + 1]));
     tc_fence_before();
     return true;
+}
+
+// Applies one TC op inside a phase (A written from this phase's registers
+// into `cur`, kappa = identity); returns false if the MMA wait gave up.
+__device__ __forceinline__ bool op_dense_tc(float2 (&v)[NR], const float2* __restrict__ bimg, float2* cur,
+                                            TcCtx& tc) {
+    unsigned char* a_hi = reinterpret_cast<unsigned char*>(cur);
+    uint4 bq[kTcBPerThread];
+    tc_load_b(bimg, bq);
+    __syncthreads();          // everyone has read `cur`, which now receives A
+    tc_write_a(v, a_hi, a_hi + 32768);
+    tc_store_b_sync(bq, tc);
+    return tc_mma_readback(v, a_hi, tc);
+}
+
+// Enters a kPhaseTcEntry phase: the registers of the previous phase go
+// straight into the A operand (in `wbuf`, whose previous readers are done) of
+// the phase's first op, whose result arrives in the phase's own layout.
+__device__ __forceinline__ bool tc_entry(float2 (&v)[NR], const TilePhase& ph, const float2* __restrict__ bimg,
+                                         float2* wbuf, TcCtx& tc) {
+    unsigned char* a_hi = reinterpret_cast<unsigned char*>(wbuf);
+    uint4 bq[kTcBPerThread];
+    tc_load_b(bimg, bq);
+    uint32_t base = 0;
+#pragma unroll
+    for (int j = 0; j < kThreadQubits; ++j)
+        if ((threadIdx.x >> j) & 1u) base ^= ph.a_thr[j];
+    uint32_t d[kRegQubits];
+#pragma unroll
+    for (int j = 0; j < kRegQubits; ++j) d[j] = ph.a_reg[j];
+#pragma unroll
+    for (int m = 0; m < NR; ++m) {
+        uint32_t off = base;
+#pragma unroll
+        for (int j = 0; j < kRegQubits; ++j)
+            if ((m >> j) & 1) off ^= d[j];
+        uint32_t hi, lo;
+        tc_split(v[m], hi, lo);
+        *reinterpret_cast<uint32_t*>(a_hi + off) = hi;
+        *reinterpret_cast<uint32_t*>(a_hi + 32768u + off) = lo;
+    }
+    tc_store_b_sync(bq, tc);
+    return tc_mma_readback(v, a_hi, tc);
 }
 
 // TOP_DIAG: the per-thread factor of the thread/memory-bit terms, the sign
@@ -584,9 +631,9 @@ __device__ __forceinline__ void op_cphase(float2 (&v)[NR], uint32_t cm, float2 p
 template <bool WIDE>
 __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, const TileOp* ops,
                                         const float2* __restrict__ mats, float2* sm, const PhaseMap& M,
-                                        bool linear, TcCtx& tc) {
+                                        bool linear, TcCtx& tc, uint32_t skip = 0) {
     const uint4* rec = reinterpret_cast<const uint4*>(ops);
-    for (uint32_t oi = ph.op_begin; oi < ph.op_end; ++oi) {
+    for (uint32_t oi = ph.op_begin + skip; oi < ph.op_end; ++oi) {
         const uint4 q0 = rec[4 * oi];
         if (q0.y & 0x00FF0000u) {          // memory controls: a thread-uniform condition
             const uint4 q1 = rec[4 * oi + 1];
@@ -841,6 +888,17 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
         for (uint32_t p = 1; p < nph && good; ++p) {
             float2* wbuf = (rbuf == xbuf) ? cur : xbuf;
             if (wbuf == xbuf) xbuf_free();
+            if constexpr (WIDE) {
+                const TilePhase& ph = phases[p];
+                if (ph.flags & kPhaseTcEntry) {
+                    const uint32_t data = reinterpret_cast<const uint4*>(ops)[4 * ph.op_begin].w;
+                    good = tc_entry(v, ph, mats + data, wbuf, tc);
+                    M = make_map(P, ph, base);
+                    rbuf = wbuf;
+                    if (good) good = run_ops<WIDE>(v, ph, ops, mats, rbuf, M, false, tc, 1);
+                    continue;
+                }
+            }
 #pragma unroll
             for (int m = 0; m < NR; ++m) wbuf[slot_of(M, m)] = v[m];
             __syncthreads();

@@ -99,12 +99,25 @@ struct TileOp {
 };
 static_assert(sizeof(TileOp) == 64, "TileOp is four 16-byte words");
 
+// TilePhase.flags
+constexpr uint8_t kPhaseTcEntry = 1;   // the phase opens with its DENSE_TC op, entered without a transpose
+
 struct TilePhase {
     uint8_t reg_pos[kRegQubits];      // register bit j <- tile-local position
     uint8_t thr_pos[kThreadQubits];   // thread bit j  <- tile-local position (lanes = j < 5)
-    uint8_t pad[3];
+    uint8_t flags;                    // kPhase* bits
+    uint8_t pad[2];
     uint32_t op_begin, op_end;
+    // kPhaseTcEntry: the previous phase's registers are written straight into
+    // the tensor-core A operand of this phase's layout (the transpose and the
+    // operand write in one step).  The byte offset of an amplitude in A is the
+    // XOR of a_thr[j] over the set bits j of the previous phase's thread index
+    // and of a_reg[j] over the set bits of its previous register index.
+    uint16_t a_thr[kThreadQubits];
+    uint16_t a_reg[kRegQubits];
+    uint16_t pad2[3];
 };
+static_assert(sizeof(TilePhase) == 56, "TilePhase layout");
 
 struct TilePass {
     uint8_t tile_pos[kTileQubits];    // tile-local position j -> memory qubit (ascending)

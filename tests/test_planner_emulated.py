@@ -64,3 +64,51 @@ def test_plain_mode_plan_is_one_step_per_instruction():
     m = circuits.random_h_rx_cx(14, 3, seed=1)
     plan = describe_plan(m, 14, "plain")
     assert len(plan["steps"]) == m.gate_count() and plan["stats"]["tile_passes"] == 0
+
+
+def _a_word_offset(ph, kappa_perm, i):
+    """Byte offset of tile-local amplitude i in the tensor-core A operand of
+    phase `ph`: row t = thread index, K index 2 kappa(m) (+1 for the
+    imaginary part), 128-byte rows with 16-byte chunks swizzled by t & 7."""
+    t = sum(((i >> p) & 1) << j for j, p in enumerate(ph["thr_pos"]))
+    m = sum(((i >> p) & 1) << j for j, p in enumerate(ph["reg_pos"]))
+    kap = sum(((m >> j) & 1) << kappa_perm[j] for j in range(5))
+    return t * 128 + (((kap >> 2) ^ (t & 7)) << 4) + (kap & 3) * 4
+
+
+@pytest.mark.parametrize("n,depth,seed", [(16, 8, 2), (18, 12, 7), (20, 24, 1234)])
+def test_tensor_core_phase_entry_offsets(n, depth, seed):
+    """Phases entered straight from the previous phase's registers: the
+    per-bit offsets (a_thr, a_reg) must send every amplitude to its word of
+    the new phase's A operand, as the tensor-core op reads it."""
+    from qlassical_b200.middleware import Middleware, TranspilerConfig
+    m = Middleware().transpile(circuits.random_rot_cz(n, depth, seed=seed),
+                               config=TranspilerConfig(max_fusion_qubits=5))
+    plan = check(m, "tiled_tc")
+    entries = 0
+    for P in plan["passes"]:
+        for k, ph in enumerate(P["phases"]):
+            if not ph["flags"] & 1:
+                continue
+            entries += 1
+            assert k > 0 and ph["ops"][0]["kind"] == 9
+            prev = P["phases"][k - 1]
+            perm = [(ph["ops"][0]["flags"] >> (3 * j)) & 7 for j in range(5)]
+            assert sorted(perm) == list(range(5))
+            seen = set()
+            for t in range(256):
+                base = 0
+                for j in range(8):
+                    if (t >> j) & 1:
+                        base ^= ph["a_thr"][j]
+                for r in range(32):
+                    off = base
+                    for j in range(5):
+                        if (r >> j) & 1:
+                            off ^= ph["a_reg"][j]
+                    i = sum(((t >> j) & 1) << p for j, p in enumerate(prev["thr_pos"]))
+                    i |= sum(((r >> j) & 1) << p for j, p in enumerate(prev["reg_pos"]))
+                    assert off == _a_word_offset(ph, perm, i)
+                    seen.add(off)
+            assert len(seen) == 8192 and max(seen) < 32768
+    assert entries > 0
