@@ -26,7 +26,7 @@ namespace qlb {
 
 namespace {
 
-constexpr uint64_t kLowMask = (uint64_t{1} << kLaneLow) - 1;  // memory qubits 0..4
+constexpr uint64_t kLowMask = (uint64_t{1} << kTileLow) - 1;  // memory qubits in every tile
 
 struct Term {            // diagonal factor exp(i*angle) on amplitudes whose qubits a (and b) are 1
     int a, b;            // -1 = absent (a < 0: a global phase)
@@ -353,29 +353,7 @@ public:
                 continue;
             }
             std::vector<uint32_t> taken, rest;
-            uint64_t T = kLowMask, blocked = 0;
-            bool stop = false;
-            for (uint32_t idx : pending) {
-                const MI& m = mi[idx];
-                if (stop || m.plain) {
-                    stop = true;
-                    rest.push_back(idx);
-                    continue;
-                }
-                if (m.touched & blocked) {
-                    blocked |= m.touched;
-                    rest.push_back(idx);
-                    continue;
-                }
-                const uint64_t nt = T | m.targets;
-                if (__builtin_popcountll(nt) > kTileQubits) {
-                    blocked |= m.touched;
-                    rest.push_back(idx);
-                    continue;
-                }
-                T = nt;
-                taken.push_back(idx);
-            }
+            const uint64_t T = pack_pass(pending, taken, rest);
             // deferred diagonal terms may ride into the next pass unless a
             // plain step (measurement, data permutation) or the end follows
             build_pass(T, taken, rest.empty() || mi[rest.front()].plain);
@@ -391,6 +369,85 @@ public:
                     std::swap(phys_to_log[p], phys_to_log[L]);
                 }
             }
+        }
+    }
+
+    // Chooses the instructions of the next pass from `pending` (program
+    // order) and returns its tile qubits.  An instruction is ready when no
+    // earlier instruction left out of the pass touches one of its qubits (it
+    // then commutes with all of them); a plain step ends the window.  Ready
+    // instructions whose targets are already tile qubits are taken at once;
+    // otherwise the ready instruction adding the fewest new tile qubits is
+    // taken (the earliest among equals), until none fits in 13.  Taken
+    // instructions keep their program order.
+    uint64_t pack_pass(const std::vector<uint32_t>& pending, std::vector<uint32_t>& taken,
+                       std::vector<uint32_t>& rest) {
+        size_t window = pending.size();
+        for (size_t i = 0; i < pending.size(); ++i)
+            if (mi[pending[i]].plain) {
+                window = i;
+                break;
+            }
+        // seeds: the first few ready instructions with targets outside the
+        // low qubits; keep the packing that takes the most target work
+        std::vector<int> seeds{-1};
+        {
+            uint64_t blocked = 0;
+            for (size_t i = 0; i < window && seeds.size() < 9; ++i) {
+                const MI& m = mi[pending[i]];
+                if (!(m.touched & blocked) && (m.targets & ~kLowMask)) seeds.push_back(static_cast<int>(i));
+                blocked |= m.touched;
+            }
+        }
+        std::vector<char> best_in;
+        uint64_t best_T = kLowMask;
+        long best_work = -1;
+        for (int seed : seeds) {
+            std::vector<char> in(pending.size(), 0);
+            uint64_t T = kLowMask;
+            if (seed >= 0) {
+                in[static_cast<size_t>(seed)] = 1;
+                T |= mi[pending[static_cast<size_t>(seed)]].targets;
+            }
+            pack_greedy(pending, window, in, T);
+            long work = 0;
+            for (size_t i = 0; i < window; ++i)
+                if (in[i]) work += 1 + 4 * __builtin_popcountll(mi[pending[i]].targets);
+            if (work > best_work) {
+                best_work = work;
+                best_in.swap(in);
+                best_T = T;
+            }
+        }
+        for (size_t i = 0; i < pending.size(); ++i) (best_in[i] ? taken : rest).push_back(pending[i]);
+        return best_T;
+    }
+    void pack_greedy(const std::vector<uint32_t>& pending, size_t window, std::vector<char>& in, uint64_t& T) {
+        for (;;) {
+            uint64_t blocked = 0;
+            int best = -1, best_add = 64;
+            for (size_t i = 0; i < window; ++i) {
+                if (in[i]) continue;
+                const MI& m = mi[pending[i]];
+                if (m.touched & blocked) {
+                    blocked |= m.touched;
+                    continue;
+                }
+                const uint64_t nt = T | m.targets;
+                const int add = __builtin_popcountll(nt & ~T);
+                if (add == 0) {
+                    in[i] = 1;
+                    continue;
+                }
+                if (__builtin_popcountll(nt) <= kTileQubits && add < best_add) {
+                    best = static_cast<int>(i);
+                    best_add = add;
+                }
+                blocked |= m.touched;
+            }
+            if (best < 0) break;
+            in[static_cast<size_t>(best)] = 1;
+            T |= mi[pending[static_cast<size_t>(best)]].targets;
         }
     }
 

@@ -34,7 +34,8 @@ constexpr int kTileQubits = 13;          // 2^13 amplitudes per tile
 constexpr int kRegQubits = 5;            // 32 amplitudes per thread
 constexpr int kThreadQubits = 8;         // 256 threads
 constexpr int kTileThreads = 1 << kThreadQubits;
-constexpr int kLaneLow = 5;              // tile positions 0..4 = memory qubits 0..4
+constexpr int kLaneLow = 5;              // lanes of the first and last phase: tile positions 0..4
+constexpr int kTileLow = 5;              // memory qubits 0..kTileLow-1 are in every tile
 constexpr uint32_t kMaxSmemOps = 160;    // ops of one pass cached in shared memory
 constexpr uint32_t kMaxSmemPhases = 24;
 
