@@ -158,7 +158,7 @@ void choose_threads(const std::vector<int>& reg, bool edge, uint8_t* thr) {
         if (!in_reg[p]) rest.push_back(p);
     std::vector<int> order;
     if (edge) {
-        order = rest;  // positions 0..4 first: lanes = memory qubits 0..4
+        order = rest;  // lowest free positions first: lanes on tile positions 0..4 where free
     } else {
         // lanes 0..3 on positions with distinct residues mod 4 (conflict-free
         // half-warp shared-memory access under the XOR fold), then the rest
@@ -570,7 +570,7 @@ private:
         {
             bool low = false;
             for (int p : phases.back().reg) low = low || p < kLaneLow;
-            if (low) phases.push_back(PhaseBuild{});  // store phase with lanes on qubits 0..4
+            if (low) phases.push_back(PhaseBuild{});  // store phase with lanes on tile positions 0..4
         }
         P.phase_begin = static_cast<uint32_t>(prog.phases.size());
         for (size_t pi = 0; pi < phases.size(); ++pi)

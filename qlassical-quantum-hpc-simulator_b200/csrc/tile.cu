@@ -1,14 +1,16 @@
 // tile.cu -- the persistent register-resident tile kernel (one launch per pass).
 //
-// One CTA per SM (256 threads, ~140 KB shared memory) walks the pass's tiles.
+// One CTA per SM (256 threads, ~220 KB shared memory) walks the pass's tiles.
 // Each tile is 2^13 complex64 amplitudes = 2^(13 - n_low) runs of 2^n_low
-// contiguous amplitudes; warp 0 streams the *next* tile into the idle
-// 64 KB buffer with cp.async.bulk (TMA bulk copies, completion counted on an
-// mbarrier) while the CTA computes the current one, so HBM reads overlap
-// compute.  A thread holds 32 amplitudes in registers; the pass's phases
-// apply their ops as register arithmetic and re-split the tile between
-// phases by transposing it through the XOR-swizzled buffer.  The last phase
-// stores straight to HBM (32 consecutive complex64 per warp request).
+// contiguous amplitudes.  Two tile buffers hold the tile being computed and
+// the next one, whose load (TMA bulk copies for long runs, cp.async for short
+// ones, completion counted on an mbarrier) was issued as soon as its buffer
+// was free, so HBM reads overlap compute.  A thread holds 32 amplitudes in
+// registers; the pass's phases apply their ops as register arithmetic and
+// re-split the tile between phases by transposing it through an XOR-swizzled
+// buffer (or, for a phase that opens with a tensor-core op, by writing the
+// registers straight into that op's operand).  The tile goes back to HBM
+// from registers (short runs) or by bulk stores from shared memory.
 // HBM traffic: 16 B per amplitude per pass, however many gates the pass holds.
 //
 // Every mbarrier wait is bounded; on expiry the CTA raises *err, waits (also
@@ -927,7 +929,7 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
             if (next + gridDim.x < ntiles) issue_load(next + gridDim.x, b);
         } else {
             // Short runs: store from registers (the last phase's lanes are
-            // memory qubits 0..4, so a warp writes 256 contiguous bytes).
+            // tile positions 0..4, so a warp writes runs of >= 64 contiguous bytes).
             __syncthreads();             // every thread is done with cur
             fence_proxy_async();         // ... before the async-proxy writes of the next load
             if (next + gridDim.x < ntiles) issue_load(next + gridDim.x, b);

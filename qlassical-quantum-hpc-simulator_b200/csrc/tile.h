@@ -2,8 +2,11 @@
 // (tile.cpp) and the sm_100a tile kernel (tile.cu).
 //
 // A *pass* is one HBM round trip.  A tile is 2^13 amplitudes whose index
-// bits are 13 memory qubits, always including qubits 0..4 (so global
-// accesses are runs of >= 256 contiguous bytes).  A persistent CTA (256
+// bits are 13 memory qubits, always including qubits 0..2 (so global
+// accesses are runs of >= 64 contiguous bytes, whole DRAM sectors; fewer
+// fixed qubits leave more room for the pass's own, hence fewer passes).
+// Tile-local positions are the tile's qubits in ascending order; the first
+// and last phase put the lanes on positions 0..4.  A persistent CTA (256
 // threads, one per SM) walks the tiles: while it computes tile i in
 // registers, the TMA engine (cp.async.bulk, mbarrier-tracked) streams tile
 // i+1 into a second 64 KB shared-memory buffer.  Inside a tile, a thread
@@ -35,7 +38,7 @@ constexpr int kRegQubits = 5;            // 32 amplitudes per thread
 constexpr int kThreadQubits = 8;         // 256 threads
 constexpr int kTileThreads = 1 << kThreadQubits;
 constexpr int kLaneLow = 5;              // lanes of the first and last phase: tile positions 0..4
-constexpr int kTileLow = 5;              // memory qubits 0..kTileLow-1 are in every tile
+constexpr int kTileLow = 3;              // memory qubits 0..kTileLow-1 are in every tile
 constexpr uint32_t kMaxSmemOps = 160;    // ops of one pass cached in shared memory
 constexpr uint32_t kMaxSmemPhases = 24;
 
@@ -123,7 +126,7 @@ static_assert(sizeof(TilePhase) == 56, "TilePhase layout");
 struct TilePass {
     uint8_t tile_pos[kTileQubits];    // tile-local position j -> memory qubit (ascending)
     uint8_t n_out;                    // number of non-tile qubits
-    uint8_t n_low;                    // tile_pos[j] == j for j < n_low (>= 5): TMA chunk = 2^n_low amps
+    uint8_t n_low;                    // tile_pos[j] == j for j < n_low (>= kTileLow): runs of 2^n_low amps
     uint8_t has_tc;                   // kernel features the pass needs (kPassTensorCores | kPassWide)
     uint8_t out_mem[40];              // non-tile memory qubits, ascending
     uint32_t phase_begin, phase_end;
