@@ -1201,11 +1201,21 @@ private:
             words(bits(b.x), bits(b.y), 0u, 0u);
         }
         for (const auto& x : S) words(static_cast<uint32_t>(x.first), static_cast<uint32_t>(x.first >> 32), x.second, 0u);
-        for (const G& g : Gs) {
-            const float2 a = f2(g.p1);
-            words(static_cast<uint32_t>(g.cmem), static_cast<uint32_t>(g.cmem >> 32), g.cm, 0u);
-            words(bits(a.x), bits(a.y), 0u, 0u);
+        // G terms by register mask (Gs is sorted by cm): a header {cm, count}
+        // per group, then its terms {u64 mem mask, float2 phase}, 16 B each
+        uint32_t n_groups = 0;
+        for (size_t g = 0; g < Gs.size();) {
+            size_t e = g;
+            while (e < Gs.size() && Gs[e].cm == Gs[g].cm) ++e;
+            words(Gs[g].cm, static_cast<uint32_t>(e - g), 0u, 0u);
+            for (size_t k = g; k < e; ++k) {
+                const float2 a = f2(Gs[k].p1);
+                words(static_cast<uint32_t>(Gs[k].cmem), static_cast<uint32_t>(Gs[k].cmem >> 32), bits(a.x), bits(a.y));
+            }
+            ++n_groups;
+            g = e;
         }
+        op.ctrl_reg = n_groups;
         prog.ops.push_back(op);
     }
 

@@ -535,13 +535,37 @@ __device__ __forceinline__ bool tc_entry(float2 (&v)[NR], const TilePhase& ph, c
     return tc_mma_readback(v, a_hi, tc);
 }
 
+// A factor f on the amplitudes whose register index contains mask cm: folded
+// into the thread-wide factor (cm = 0) or the factor of one register bit (a
+// single bit, the common case: a controlled phase between a register qubit
+// and any other), applied later with loops whose structure is fixed at
+// compile time; several bits are applied now.
+__device__ __forceinline__ void diag_fold(float2 (&v)[NR], float2& T, float2 (&F)[kRegQubits], uint32_t cm,
+                                          float2 f) {
+    if (cm == 0u) {
+        T = cmul(T, f);
+    } else if ((cm & (cm - 1u)) == 0u) {
+#pragma unroll
+        for (int j = 0; j < kRegQubits; ++j)
+            if (cm == (1u << j)) F[j] = cmul(F[j], f);
+    } else {
+#pragma unroll
+        for (int m = 0; m < NR; ++m)
+            if ((static_cast<uint32_t>(m) & cm) == cm) v[m] = cmul(v[m], f);
+    }
+}
+
 // TOP_DIAG: the per-thread factor of the thread/memory-bit terms, the sign
-// mask of the mixed pi terms, then one complex multiply per amplitude.
+// mask of the mixed pi terms, the per-register-bit factors of the mixed
+// terms, then one complex multiply per amplitude and factor.
 __device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* __restrict__ tab, uint32_t flags,
                                         uint32_t n_t, uint32_t n_s, uint32_t n_g, uint64_t gt) {
     const uint32_t has_r = flags & 1u;
     const float2* q = tab + (has_r ? 32 : 0);
     float2 T = make_float2(1.f, 0.f);
+    float2 F[kRegQubits];
+#pragma unroll
+    for (int j = 0; j < kRegQubits; ++j) F[j] = make_float2(1.f, 0.f);
     if (flags & 2u) {
         T = __ldg(q + threadIdx.x);
         q += 256;
@@ -557,7 +581,7 @@ __device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* __restric
     const float2* gtab = q;
     q += 256 * n_gt;
     const uint4* p = reinterpret_cast<const uint4*>(q);
-#pragma unroll 2
+#pragma unroll 4
     for (uint32_t t = 0; t < n_t; ++t) {
         const uint4 w0 = __ldg(p + 2 * t), w1 = __ldg(p + 2 * t + 1);
         const uint64_t c = (static_cast<uint64_t>(w0.y) << 32) | w0.x;
@@ -574,12 +598,39 @@ __device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* __restric
         smask ^= ((gt & c) == c) ? w.z : 0u;
     }
     p += n_s;
+    for (uint32_t g = 0; g < n_gt; ++g) {
+        const float2 f = __ldg(gtab + 256 * g + threadIdx.x);
+        if (f.x == 1.f && f.y == 0.f) continue;
+        diag_fold(v, T, F, __ldg(gcm + g), f);
+    }
+    // G groups (one register mask each): the group's factor is a product over
+    // its terms (independent loads, unrolled), folded once.
+    for (uint32_t g = 0; g < n_g; ++g) {
+        const uint4 h = __ldg(p);
+        ++p;
+        float2 gf = make_float2(1.f, 0.f);
+#pragma unroll 4
+        for (uint32_t k = 0; k < h.y; ++k) {
+            const uint4 w = __ldg(p + k);
+            const uint64_t c = (static_cast<uint64_t>(w.y) << 32) | w.x;
+            if ((gt & c) == c) gf = cmul(gf, make_float2(__uint_as_float(w.z), __uint_as_float(w.w)));
+        }
+        p += h.y;
+        if (gf.x != 1.f || gf.y != 0.f) diag_fold(v, T, F, h.x, gf);
+    }
     if (has_r) {
 #pragma unroll
         for (int m = 0; m < NR; ++m) v[m] = cmul(v[m], cmul(T, __ldg(tab + m)));
     } else if (T.x != 1.f || T.y != 0.f) {
 #pragma unroll
         for (int m = 0; m < NR; ++m) v[m] = cmul(v[m], T);
+    }
+#pragma unroll
+    for (int j = 0; j < kRegQubits; ++j) {
+        if (F[j].x == 1.f && F[j].y == 0.f) continue;
+#pragma unroll
+        for (int m = 0; m < NR; ++m)
+            if ((m >> j) & 1) v[m] = cmul(v[m], F[j]);
     }
     if (smask) {
 #pragma unroll
@@ -588,35 +639,6 @@ __device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* __restric
             v[m].x = __uint_as_float(__float_as_uint(v[m].x) ^ sgn);
             v[m].y = __uint_as_float(__float_as_uint(v[m].y) ^ sgn);
         }
-    }
-    for (uint32_t g = 0; g < n_gt; ++g) {
-        const float2 f = __ldg(gtab + 256 * g + threadIdx.x);
-        if (f.x == 1.f && f.y == 0.f) continue;
-        const uint32_t cm = __ldg(gcm + g);
-#pragma unroll
-        for (int m = 0; m < NR; ++m)
-            if ((static_cast<uint32_t>(m) & cm) == cm) v[m] = cmul(v[m], f);
-    }
-    // G terms arrive grouped by register mask: the factors of a group are
-    // multiplied per thread, then applied once.
-    float2 gf = make_float2(1.f, 0.f);
-    uint32_t gcur = 0;
-    for (uint32_t g = 0; g <= n_g; ++g) {
-        uint4 w0 = make_uint4(0u, 0u, 0xFFFFFFFFu, 0u), w1 = make_uint4(0u, 0u, 0u, 0u);
-        if (g < n_g) {
-            w0 = __ldg(p + 2 * g);
-            w1 = __ldg(p + 2 * g + 1);
-        }
-        if (g > 0 && w0.z != gcur && (gf.x != 1.f || gf.y != 0.f)) {
-#pragma unroll
-            for (int m = 0; m < NR; ++m)
-                if ((static_cast<uint32_t>(m) & gcur) == gcur) v[m] = cmul(v[m], gf);
-        }
-        if (g == n_g) break;
-        if (w0.z != gcur || g == 0) gf = make_float2(1.f, 0.f);
-        gcur = w0.z;
-        const uint64_t c = (static_cast<uint64_t>(w0.y) << 32) | w0.x;
-        if ((gt & c) == c) gf = cmul(gf, make_float2(__uint_as_float(w1.x), __uint_as_float(w1.y)));
     }
 }
 

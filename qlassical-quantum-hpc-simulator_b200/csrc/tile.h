@@ -88,7 +88,9 @@ __host__ __device__ constexpr uint32_t reg_pair_index(uint32_t a, uint32_t b) { 
 //     n & 0xFFFF  T terms, 32 B each: {u64 mem mask, float2 p1, float2 p0}: a thread whose
 //                 index has every mask bit set multiplies by p1, otherwise by p0
 //     n >> 16     S terms, 16 B each: {u64 mem mask, u32 register pattern, 0}: sign flips
-//     ctrl_reg    G terms, 32 B each: {u64 mem mask, u32 register mask, 0, float2 phase, 0, 0}
+//     ctrl_reg    G groups: a 16 B header {u32 register mask, u32 count, 0, 0}, then count
+//                 terms of 16 B {u64 mem mask, float2 phase}: the amplitudes whose index has
+//                 every mem-mask bit and whose register index contains the mask get the phase
 struct TileOp {
     uint16_t code;          // TileOpCode
     uint8_t kind, k;        // TileOpKind; DENSE: k

@@ -150,13 +150,15 @@ def apply_diag(st, n, mq, op, words, tq):
         hit = ((idx & c) == c) & (((pat >> reg) & 1) == 1)
         fac[hit] *= -1.0
         pos += 4
-    for _ in range(n_g):
-        c = int(w[pos]) | (int(w[pos + 1]) << 32)
-        cm = int(w[pos + 2])
-        ph = f[pos + 4] + 1j * f[pos + 5]
-        hit = ((idx & c) == c) & ((reg & cm) == cm)
-        fac[hit] *= ph
-        pos += 8
+    for _ in range(n_g):                      # groups: header {cm, count}, then count terms {mask, phase}
+        cm, cnt = int(w[pos]), int(w[pos + 1])
+        pos += 4
+        for _ in range(cnt):
+            c = int(w[pos]) | (int(w[pos + 1]) << 32)
+            ph = f[pos + 2] + 1j * f[pos + 3]
+            hit = ((idx & c) == c) & ((reg & cm) == cm)
+            fac[hit] *= ph
+            pos += 4
     st *= fac
 
 
