@@ -350,13 +350,14 @@ __device__ __forceinline__ void op_dense5(float2 (&v)[NR], const float2* __restr
 // apart (SBO).  B is K-major without swizzle: 8 x 16 B core matrices,
 // LBO = 128 B between the K chunks of one row group, SBO = 1024 B between
 // 8-row groups.  D column n of row t is read back by thread t.
-constexpr uint32_t kTcCols = 128;
+constexpr uint32_t kTcCols = 256;               // per M-block: D1 (64 columns) | D2 (64 columns)
 constexpr uint32_t kTcBBytes = 16384;          // B hi (8 KB) + B lo (8 KB)
-constexpr uint32_t kTcIdesc = (1u << 4)        // D format F32
-                              | (1u << 7)      // A format BF16
-                              | (1u << 10)     // B format BF16
-                              | ((64u >> 3) << 17)    // N = 64
-                              | ((128u >> 4) << 24);  // M = 128
+constexpr uint32_t kTcIdescBase = (1u << 4)    // D format F32
+                                  | (1u << 7)  // A format BF16
+                                  | (1u << 10) // B format BF16
+                                  | ((128u >> 4) << 24);  // M = 128
+constexpr uint32_t kTcIdesc64 = kTcIdescBase | ((64u >> 3) << 17);     // N = 64
+constexpr uint32_t kTcIdesc128 = kTcIdescBase | ((128u >> 3) << 17);   // N = 128  // M = 128
 
 // B: no swizzle, LBO 128 B, SBO 1024 B.
 __device__ __forceinline__ uint64_t umma_desc_b(uint32_t smem_addr) {
@@ -398,12 +399,12 @@ __device__ __forceinline__ void tc_write_a(const float2 (&v)[NR], unsigned char*
     }
 }
 
-__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-        ::"r"(d_tmem), "l"(a), "l"(b), "r"(kTcIdesc), "r"(accumulate)
+        ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
         : "memory");
 }
 __device__ __forceinline__ void tc_commit(uint64_t* bar) {
@@ -413,24 +414,17 @@ __device__ __forceinline__ void tc_commit(uint64_t* bar) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tc_ld_row(uint32_t taddr, uint32_t (&r)[64]) {
+__device__ __forceinline__ void tc_ld_32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
         "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, "
-        "%32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, "
-        "%48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];"
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
           "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
-          "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
-          "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
-          "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
-          "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr)
         : "memory");
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
 struct TcCtx {
@@ -461,22 +455,26 @@ __device__ __forceinline__ void tc_store_b_sync(const uint4 (&bq)[kTcBPerThread]
     tc_fence_before();
     __syncthreads();
 }
-// Thread 0 issues the 24 MMAs of the op (A at a_hi, a_hi + 32 KB); everyone
-// waits for them and reads its row of D back into v (this phase's layout).
-// Returns false if the wait gave up (all threads agree).
+// Thread 0 issues the 16 MMAs of the op (A at a_hi, a_hi + 32 KB): per M-block
+// of 128 rows, A_hi x [B_hi | B_lo] as N = 128 into D1 | D2, then A_lo x B_hi
+// accumulated into D1; everyone waits for them and reads its row of
+// D1 + D2 back into v (this phase's layout).  Returns false if the wait gave
+// up (all threads agree).
 __device__ __forceinline__ bool tc_mma_readback(float2 (&v)[NR], const unsigned char* a_hi, TcCtx& tc) {
     if (threadIdx.x == 0) {
         tc_fence_after();
-        const uint32_t ahi = smem_u32(a_hi), alo = ahi + 32768u, bhi = smem_u32(tc.sb), blo = bhi + 8192u;
-        const uint32_t as[3] = {ahi, ahi, alo}, bs[3] = {bhi, blo, bhi};
+        const uint32_t ahi = smem_u32(a_hi), alo = ahi + 32768u, bhi = smem_u32(tc.sb);
 #pragma unroll
-        for (uint32_t mb = 0; mb < 2; ++mb)
+        for (uint32_t mb = 0; mb < 2; ++mb) {
+            const uint32_t d = tc.tmem + mb * 128u;
 #pragma unroll
-            for (int p = 0; p < 3; ++p)
+            for (uint32_t s = 0; s < 4; ++s)
+                tc_mma(d, umma_desc_a(ahi + mb * 16384u + s * 32u), umma_desc_b(bhi + s * 256u), kTcIdesc128,
+                       s > 0 ? 1u : 0u);
 #pragma unroll
-                for (uint32_t s = 0; s < 4; ++s)
-                    tc_mma(tc.tmem + mb * 64u, umma_desc_a(as[p] + mb * 16384u + s * 32u),
-                           umma_desc_b(bs[p] + s * 256u), (p > 0 || s > 0) ? 1u : 0u);
+            for (uint32_t s = 0; s < 4; ++s)
+                tc_mma(d, umma_desc_a(alo + mb * 16384u + s * 32u), umma_desc_b(bhi + s * 256u), kTcIdesc64, 1u);
+        }
         tc_commit(tc.bar);
     }
     const bool ok = mbar_wait_bounded(tc.bar, tc.uses & 1u);
@@ -484,10 +482,18 @@ __device__ __forceinline__ bool tc_mma_readback(float2 (&v)[NR], const unsigned 
     if (__syncthreads_or(!ok)) return false;
     tc_fence_after();
     const uint32_t w = threadIdx.x >> 5;
-    uint32_t r[64];
-    tc_ld_row(tc.tmem + (((w & 3u) * 32u) << 16) + (w >> 2) * 64u, r);
+    const uint32_t row = tc.tmem + (((w & 3u) * 32u) << 16) + (w >> 2) * 128u;
 #pragma unroll
-    for (int c = 0; c < NR; ++c) v[c] = make_float2(__uint_as_float(r[2 * c]), __uint_as_float(r[2 * c + 1]));
+    for (uint32_t h = 0; h < 2; ++h) {
+        uint32_t r1[32], r2[32];
+        tc_ld_32(row + h * 32u, r1);
+        tc_ld_32(row + 64u + h * 32u, r2);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int c = 0; c < 16; ++c)
+            v[16 * h + c] = make_float2(__uint_as_float(r1[2 * c]) + __uint_as_float(r2[2 * c]),
+                                        __uint_as_float(r1[2 * c + 1]) + __uint_as_float(r2[2 * c + 1]));
+    }
     tc_fence_before();
     return true;
 }
