@@ -587,7 +587,7 @@ __device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* __restric
     const float2* gtab = q;
     q += 256 * n_gt;
     const uint4* p = reinterpret_cast<const uint4*>(q);
-#pragma unroll 4
+#pragma unroll 2
     for (uint32_t t = 0; t < n_t; ++t) {
         const uint4 w0 = __ldg(p + 2 * t), w1 = __ldg(p + 2 * t + 1);
         const uint64_t c = (static_cast<uint64_t>(w0.y) << 32) | w0.x;
@@ -631,12 +631,14 @@ __device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* __restric
 #pragma unroll
         for (int m = 0; m < NR; ++m) v[m] = cmul(v[m], T);
     }
+    if (n_gt | n_g) {
 #pragma unroll
-    for (int j = 0; j < kRegQubits; ++j) {
-        if (F[j].x == 1.f && F[j].y == 0.f) continue;
+        for (int j = 0; j < kRegQubits; ++j) {
+            if (F[j].x == 1.f && F[j].y == 0.f) continue;
 #pragma unroll
-        for (int m = 0; m < NR; ++m)
-            if ((m >> j) & 1) v[m] = cmul(v[m], F[j]);
+            for (int m = 0; m < NR; ++m)
+                if ((m >> j) & 1) v[m] = cmul(v[m], F[j]);
+        }
     }
     if (smask) {
 #pragma unroll
