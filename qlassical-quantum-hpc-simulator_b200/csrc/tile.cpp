@@ -529,8 +529,10 @@ private:
                 for (uint32_t b = 0; b < n_; ++b)
                     if (m.targets & bitm(b)) tl.push_back(local_of[b]);
                 bool ok = true;
+                // the first phase reads the tile as loaded: its lanes keep the
+                // tile's low qubits 0..2 (runs of 8 amplitudes per 8 lanes)
                 if (first)
-                    for (int p : tl) ok = ok && p >= kLaneLow;
+                    for (int p : tl) ok = ok && p >= kTileLow;
                 const bool dense = !m.diag && m.k >= 3 && (m.type == QLB_UNITARY || m.type == QLB_FUSED_BLOCK);
                 std::vector<int> mdq;
                 if (dense) {
@@ -569,7 +571,7 @@ private:
         if (phases.empty()) phases.push_back(PhaseBuild{});
         {
             bool low = false;
-            for (int p : phases.back().reg) low = low || p < kLaneLow;
+            for (int p : phases.back().reg) low = low || p < kTileLow;
             if (low) phases.push_back(PhaseBuild{});  // store phase with lanes on tile positions 0..4
         }
         P.phase_begin = static_cast<uint32_t>(prog.phases.size());
