@@ -6,15 +6,16 @@
 // accesses are runs of >= 64 contiguous bytes, whole DRAM sectors; fewer
 // fixed qubits leave more room for the pass's own, hence fewer passes).
 // Tile-local positions are the tile's qubits in ascending order; the first
-// and last phase put the lanes on positions 0..4.  A persistent CTA (256
-// threads, one per SM) walks the tiles: while it computes tile i in
-// registers, the TMA engine (cp.async.bulk, mbarrier-tracked) streams tile
-// i+1 into a second 64 KB shared-memory buffer.  Inside a tile, a thread
+// and last phase put the lanes on positions 0..4 (they need only 0..2).  A
+// persistent CTA (256 threads, one per SM) walks the tiles: while it computes
+// tile i in registers, tile i+1 streams into a second 64 KB shared-memory
+// buffer (TMA bulk copies or cp.async, mbarrier-tracked).  Inside a tile, a thread
 // holds 32 amplitudes in registers: five tile qubits are "register qubits"
 // (a gate on them is register arithmetic), the other eight index the
 // thread.  A *phase* fixes that split; between phases the tile is
 // transposed through XOR-swizzled shared memory (bank-conflict free for the
-// chosen lane qubits).  The last phase stores straight to HBM.
+// chosen lane qubits).  The last phase stores to HBM from registers or by
+// bulk stores from shared memory.
 //
 // Diagonal instructions (Z, S, RZ, CZ, CP, diagonal UNITARY) and controls
 // never need their qubit in registers: their effect depends only on the
