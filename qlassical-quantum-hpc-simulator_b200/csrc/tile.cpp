@@ -378,30 +378,49 @@ public:
     // then commutes with all of them); a plain step ends the window.  Ready
     // instructions whose targets are already tile qubits are taken at once;
     // otherwise the ready instruction adding the fewest new tile qubits is
-    // taken (the earliest among equals), until none fits in 13.  Taken
-    // instructions keep their program order.
+    // taken (the earliest among equals), until none fits in 13.  The packing
+    // kept is the best of several such greedy packings, each seeded with one
+    // of the first ready instructions and scored (for streams of up to
+    // kLookaheadMaxPending instructions) together with the best packing of
+    // the pass after it.  Taken instructions keep their program order.
     uint64_t pack_pass(const std::vector<uint32_t>& pending, std::vector<uint32_t>& taken,
                        std::vector<uint32_t>& rest) {
+        std::vector<char> in;
+        // the look-ahead costs ~seeds^2 greedy packings: short streams only
+        const uint64_t T = pack_best(pending, in, pending.size() <= kLookaheadMaxPending ? 1 : 0);
+        for (size_t i = 0; i < pending.size(); ++i) (in[i] ? taken : rest).push_back(pending[i]);
+        return T;
+    }
+    // Work of a packing: instructions plus 4 per target qubit.
+    long pack_work(const std::vector<uint32_t>& pending, const std::vector<char>& in) const {
+        long work = 0;
+        for (size_t i = 0; i < in.size(); ++i)
+            if (in[i]) work += 1 + 4 * __builtin_popcountll(mi[pending[i]].targets);
+        return work;
+    }
+    // The packing of the next pass: the best of the greedy packings seeded
+    // with each of the first ready instructions, scored by its own work plus
+    // (depth > 0) the work of the best packing of the pass after it.
+    static constexpr size_t kLookaheadMaxPending = 768;
+    static constexpr size_t kSeeds = 12;
+    uint64_t pack_best(const std::vector<uint32_t>& pending, std::vector<char>& best_in, int depth) {
         size_t window = pending.size();
         for (size_t i = 0; i < pending.size(); ++i)
             if (mi[pending[i]].plain) {
                 window = i;
                 break;
             }
-        // seeds: the first few ready instructions with targets outside the
-        // low qubits; keep the packing that takes the most target work
         std::vector<int> seeds{-1};
         {
             uint64_t blocked = 0;
-            for (size_t i = 0; i < window && seeds.size() < 9; ++i) {
+            for (size_t i = 0; i < window && seeds.size() < kSeeds; ++i) {
                 const MI& m = mi[pending[i]];
                 if (!(m.touched & blocked) && (m.targets & ~kLowMask)) seeds.push_back(static_cast<int>(i));
                 blocked |= m.touched;
             }
         }
-        std::vector<char> best_in;
         uint64_t best_T = kLowMask;
-        long best_work = -1;
+        long best_score = -1;
         for (int seed : seeds) {
             std::vector<char> in(pending.size(), 0);
             uint64_t T = kLowMask;
@@ -410,16 +429,23 @@ public:
                 T |= mi[pending[static_cast<size_t>(seed)]].targets;
             }
             pack_greedy(pending, window, in, T);
-            long work = 0;
-            for (size_t i = 0; i < window; ++i)
-                if (in[i]) work += 1 + 4 * __builtin_popcountll(mi[pending[i]].targets);
-            if (work > best_work) {
-                best_work = work;
+            long score = pack_work(pending, in);
+            if (depth > 0) {
+                std::vector<uint32_t> rest;
+                for (size_t i = 0; i < window; ++i)
+                    if (!in[i]) rest.push_back(pending[i]);
+                if (!rest.empty()) {
+                    std::vector<char> in2;
+                    pack_best(rest, in2, depth - 1);
+                    score += pack_work(rest, in2);
+                }
+            }
+            if (score > best_score) {
+                best_score = score;
                 best_in.swap(in);
                 best_T = T;
             }
         }
-        for (size_t i = 0; i < pending.size(); ++i) (best_in[i] ? taken : rest).push_back(pending[i]);
         return best_T;
     }
     void pack_greedy(const std::vector<uint32_t>& pending, size_t window, std::vector<char>& in, uint64_t& T) {
