@@ -595,11 +595,13 @@ int qlb_engine_execute(qlb_engine_t e, const qlb_gate_instr* prog, uint64_t coun
         if (count && !prog) fail(QLB_ERR_INVALID_ARG, "program is null");
         if (e->sv.dim == 0) fail(QLB_ERR_STATE, "engine has no state vector");
         for (uint64_t i = 0; i < count; ++i) validate_instr(prog[i], e->sv.n, pool);
-        std::unique_ptr<qlb_plan> p(compile_plan(*e, prog, count, pool));
+        // the plan's device image goes to a buffer the engine keeps, so a
+        // call allocates and frees no device memory once it has grown
+        std::unique_ptr<qlb_plan> p(compile_plan(*e, prog, count, pool, &e->exec_plan));
         e->stats = p->stats;
         run_plan(*e, *p);
-        // the plan's device buffer is freed when `p` goes out of scope; the
-        // kernels that read it must have finished by then
+        // the kernels that read the plan image must finish before the next
+        // call reuses the buffer
         check_cuda(cudaStreamSynchronize(e->stream), "execute sync");
         check_device_error(*e);
     });

@@ -33,6 +33,7 @@ struct qlb_plan {
     int mode = 0;
     std::vector<qlb::PlanStep> steps;
     qlb::DeviceBuffer dev;   // [passes | phases | ops | matrices]
+    const void* image = nullptr;   // the device image: dev.p, or a buffer the engine lends for one execute()
     size_t o_pass = 0, o_phase = 0, o_ops = 0, o_mat = 0;
     qlb_exec_stats stats{};
 };
@@ -56,6 +57,9 @@ struct HostPlan {
 };
 HostPlan plan_host(const PlanConfig& cfg, const qlb_gate_instr* prog, uint64_t count, const qlb_pool_view* pool);
 // Builds a plan for the engine's qubit count, mode and options.
-qlb_plan* compile_plan(qlb_engine& e, const qlb_gate_instr* prog, uint64_t count, const qlb_pool_view* pool);
+// `image`: a device buffer to hold the plan (reused across calls, e.g. by
+// execute()); nullptr: the plan owns its own.
+qlb_plan* compile_plan(qlb_engine& e, const qlb_gate_instr* prog, uint64_t count, const qlb_pool_view* pool,
+                       qlb::DeviceBuffer* image = nullptr);
 void run_plan(qlb_engine& e, const qlb_plan& p);
 }  // namespace qlb

@@ -1339,7 +1339,8 @@ HostPlan plan_host(const PlanConfig& cfg, const qlb_gate_instr* prog, uint64_t c
     return h;
 }
 
-qlb_plan* compile_plan(qlb_engine& e, const qlb_gate_instr* prog, uint64_t count, const qlb_pool_view* pool) {
+qlb_plan* compile_plan(qlb_engine& e, const qlb_gate_instr* prog, uint64_t count, const qlb_pool_view* pool,
+                       DeviceBuffer* image) {
     Planner pl(PlanConfig{e.sv.n, e.mode, e.physical_global_swap, e.tc_min_cost}, pool);
     pl.plan(prog, count);
     TileProgram& tp = pl.prog;
@@ -1362,7 +1363,8 @@ qlb_plan* compile_plan(qlb_engine& e, const qlb_gate_instr* prog, uint64_t count
         std::memcpy(h + p->o_phase, tp.phases.data(), tp.phases.size() * sizeof(TilePhase));
         std::memcpy(h + p->o_ops, tp.ops.data(), tp.ops.size() * sizeof(TileOp));
         std::memcpy(h + p->o_mat, tp.mats.data(), tp.mats.size() * sizeof(float2));
-        void* d = p->dev.ensure(total);
+        void* d = image ? image->ensure(total) : p->dev.ensure(total);
+        p->image = d;
         check_cuda(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, e.stream), "H2D plan");
     } catch (...) {
         delete p;
@@ -1519,7 +1521,7 @@ void run_plan(qlb_engine& e, const qlb_plan& p) {
         e.err_flag.ensure(256);
         check_cuda(cudaMemsetAsync(e.err_flag.p, 0, sizeof(int), e.stream), "clear error flag");
     }
-    const char* d = static_cast<const char*>(p.dev.p);
+    const char* d = static_cast<const char*>(p.image);
     const float2* mats = reinterpret_cast<const float2*>(d + p.o_mat);
     for (const PlanStep& st : p.steps) {
         switch (st.kind) {
