@@ -1244,6 +1244,17 @@ private:
             g = e;
         }
         op.ctrl_reg = n_groups;
+        // Read from global memory, the op's tables and term lists cost a chain
+        // of dependent L2 round trips (about one per table, per group and per
+        // two T terms); when that chain is long the kernel first copies the
+        // data (whole 16-byte words) into shared memory in one round trip and
+        // two barriers.  m[0].x = the word count then, else 0.
+        if (prog.mats.size() & 1) prog.mats.push_back(make_float2(0.f, 0.f));
+        const uint32_t n_words = static_cast<uint32_t>((prog.mats.size() - op.data) / 2);
+        const size_t chain = ((op.flags & 6u) ? 1 : 0) + (has_r ? 1 : 0) + gcm.size() + 2 * n_groups +
+                             (T.size() + 1) / 2 + (S.size() + 3) / 4;
+        const uint32_t stage_words = (chain >= 4 && n_words <= kDiagStageWords) ? n_words : 0u;
+        std::memcpy(&op.m[0].x, &stage_words, 4);
         prog.ops.push_back(op);
     }
 

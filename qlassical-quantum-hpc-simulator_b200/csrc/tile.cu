@@ -561,10 +561,43 @@ __device__ __forceinline__ void diag_fold(float2 (&v)[NR], float2& T, float2 (&F
     }
 }
 
+// Copies a DIAG op's data (n_words 16-byte words, at most kDiagStageWords) into the
+// B staging area: each thread has two words in flight, so up to 8 KB cost one
+// L2 round trip instead of the chain of dependent loads the op's tables and
+// term lists would take from global memory.  The area is free:
+// a tensor-core op's MMAs have completed when it returns, and a DIAG op that
+// staged ends with a barrier.
+static_assert(kDiagStageWords * 16u <= kTcBBytes, "DIAG staging fits the B staging area");
+__device__ __forceinline__ const float2* diag_stage(const float2* __restrict__ src, uint32_t n_words,
+                                                   unsigned char* sb) {
+    const uint4* s4 = reinterpret_cast<const uint4*>(src);
+    uint4* d4 = reinterpret_cast<uint4*>(sb);
+    constexpr uint32_t kPer = 2;      // words in flight per thread (registers are scarce here)
+#pragma unroll 1
+    for (uint32_t b = 0; b < n_words; b += kPer * NT) {
+        uint4 t[kPer];
+#pragma unroll
+        for (uint32_t i = 0; i < kPer; ++i) {
+            const uint32_t k = b + i * NT + threadIdx.x;
+            if (k < n_words) t[i] = __ldg(s4 + k);
+        }
+#pragma unroll
+        for (uint32_t i = 0; i < kPer; ++i) {
+            const uint32_t k = b + i * NT + threadIdx.x;
+            if (k < n_words) d4[k] = t[i];
+        }
+    }
+    __syncthreads();
+    return reinterpret_cast<const float2*>(sb);
+}
+
 // TOP_DIAG: the per-thread factor of the thread/memory-bit terms, the sign
 // mask of the mixed pi terms, the per-register-bit factors of the mixed
-// terms, then one complex multiply per amplitude and factor.
-__device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* __restrict__ tab, uint32_t flags,
+// terms, then one complex multiply per amplitude and factor.  `tab` is the
+// op's data in shared memory (staged by diag_stage) or in global memory:
+// plain (generic) loads serve both (a copy of this code per address space
+// measured slower: the kernels' code grows).
+__device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* tab, uint32_t flags,
                                         uint32_t n_t, uint32_t n_s, uint32_t n_g, uint64_t gt) {
     const uint32_t has_r = flags & 1u;
     const float2* q = tab + (has_r ? 32 : 0);
@@ -573,12 +606,12 @@ __device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* __restric
 #pragma unroll
     for (int j = 0; j < kRegQubits; ++j) F[j] = make_float2(1.f, 0.f);
     if (flags & 2u) {
-        T = __ldg(q + threadIdx.x);
+        T = q[threadIdx.x];
         q += 256;
     }
     uint32_t smask = 0;
     if (flags & 4u) {
-        smask = __ldg(reinterpret_cast<const uint32_t*>(q) + threadIdx.x);
+        smask = reinterpret_cast<const uint32_t*>(q)[threadIdx.x];
         q += 128;
     }
     const uint32_t n_gt = (flags >> 8) & 0xFFu;
@@ -589,7 +622,7 @@ __device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* __restric
     const uint4* p = reinterpret_cast<const uint4*>(q);
 #pragma unroll 2
     for (uint32_t t = 0; t < n_t; ++t) {
-        const uint4 w0 = __ldg(p + 2 * t), w1 = __ldg(p + 2 * t + 1);
+        const uint4 w0 = p[2 * t], w1 = p[2 * t + 1];
         const uint64_t c = (static_cast<uint64_t>(w0.y) << 32) | w0.x;
         const bool on = (gt & c) == c;
         const float2 f = on ? make_float2(__uint_as_float(w0.z), __uint_as_float(w0.w))
@@ -599,25 +632,25 @@ __device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* __restric
     p += 2 * n_t;
 #pragma unroll 4
     for (uint32_t t = 0; t < n_s; ++t) {
-        const uint4 w = __ldg(p + t);
+        const uint4 w = p[t];
         const uint64_t c = (static_cast<uint64_t>(w.y) << 32) | w.x;
         smask ^= ((gt & c) == c) ? w.z : 0u;
     }
     p += n_s;
     for (uint32_t g = 0; g < n_gt; ++g) {
-        const float2 f = __ldg(gtab + 256 * g + threadIdx.x);
+        const float2 f = gtab[256 * g + threadIdx.x];
         if (f.x == 1.f && f.y == 0.f) continue;
-        diag_fold(v, T, F, __ldg(gcm + g), f);
+        diag_fold(v, T, F, gcm[g], f);
     }
     // G groups (one register mask each): the group's factor is a product over
     // its terms (independent loads, unrolled), folded once.
     for (uint32_t g = 0; g < n_g; ++g) {
-        const uint4 h = __ldg(p);
+        const uint4 h = *p;
         ++p;
         float2 gf = make_float2(1.f, 0.f);
 #pragma unroll 4
         for (uint32_t k = 0; k < h.y; ++k) {
-            const uint4 w = __ldg(p + k);
+            const uint4 w = p[k];
             const uint64_t c = (static_cast<uint64_t>(w.y) << 32) | w.x;
             if ((gt & c) == c) gf = cmul(gf, make_float2(__uint_as_float(w.z), __uint_as_float(w.w)));
         }
@@ -626,7 +659,7 @@ __device__ __forceinline__ void op_diag(float2 (&v)[NR], const float2* __restric
     }
     if (has_r) {
 #pragma unroll
-        for (int m = 0; m < NR; ++m) v[m] = cmul(v[m], cmul(T, __ldg(tab + m)));
+        for (int m = 0; m < NR; ++m) v[m] = cmul(v[m], cmul(T, tab[m]));
     } else if (T.x != 1.f || T.y != 0.f) {
 #pragma unroll
         for (int m = 0; m < NR; ++m) v[m] = cmul(v[m], T);
@@ -711,9 +744,14 @@ __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, co
     QLB_RX_CASE(0) QLB_RX_CASE(1) QLB_RX_CASE(2) QLB_RX_CASE(3) QLB_RX_CASE(4)                        \
     QLB_U1_CASE(0) QLB_U1_CASE(1) QLB_U1_CASE(2) QLB_U1_CASE(3) QLB_U1_CASE(4)                        \
     QLB_X_CASE(0) QLB_X_CASE(1) QLB_X_CASE(2) QLB_X_CASE(3) QLB_X_CASE(4)                             \
-    case OPC_DIAG:                                                                                    \
-        op_diag(v, mats + data, rec[4 * oi + 1].x, rec[4 * oi + 1].y & 0xFFFFu, rec[4 * oi + 1].y >> 16, cm, M.gt); \
-        break;                                                                                        \
+    case OPC_DIAG: {                                                                                  \
+        const uint32_t n_words = rec[4 * oi + 2].x;    /* 0: read from global memory */              \
+        const uint4 q1 = rec[4 * oi + 1];                                                             \
+        const bool staged = n_words - 1u < kDiagStageWords;                                           \
+        const float2* tab = staged ? diag_stage(mats + data, n_words, tc.sb) : mats + data;           \
+        op_diag(v, tab, q1.x, q1.y & 0xFFFFu, q1.y >> 16, cm, M.gt);                                  \
+        if (staged) __syncthreads();   /* the staging area is free again */                           \
+    } break;                                                                                          \
     case OPC_CPHASE:                                                                                  \
         op_cphase(v, cm, f2(rec[4 * oi + 2].x, rec[4 * oi + 2].y));                                  \
         break;

@@ -42,6 +42,7 @@ constexpr int kLaneLow = 5;              // lanes of the first and last phase: t
 constexpr int kTileLow = 3;              // memory qubits 0..kTileLow-1 are in every tile
 constexpr uint32_t kMaxSmemOps = 160;    // ops of one pass cached in shared memory
 constexpr uint32_t kMaxSmemPhases = 24;
+constexpr uint32_t kDiagStageWords = 1024; // 16-byte words of DIAG data staged in shared memory (16 KB)
 
 enum TileOpKind : uint8_t {
     TOP_U1 = 1,       // complex 2x2 on register bit r0 (controls: ctrl_reg / ctrl_mem)
@@ -92,6 +93,9 @@ __host__ __device__ constexpr uint32_t reg_pair_index(uint32_t a, uint32_t b) { 
 //     ctrl_reg    G groups: a 16 B header {u32 register mask, u32 count, 0, 0}, then count
 //                 terms of 16 B {u64 mem mask, float2 phase}: the amplitudes whose index has
 //                 every mem-mask bit and whose register index contains the mask get the phase
+//     m[0].x      (u32 bits) 0, or the data's length in 16-byte words when the kernel is to
+//                 stage it in shared memory first; the data starts on a 16-byte boundary
+//                 and is padded to whole words
 struct TileOp {
     uint16_t code;          // TileOpCode
     uint8_t kind, k;        // TileOpKind; DENSE: k
