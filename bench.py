@@ -368,6 +368,32 @@ def run_ours(args):
                      "max_abs_diff": float(np.max(np.abs(a_tc - a_ref))),
                      "sampled_infidelity": float(1.0 - abs(ip) ** 2 / (np.vdot(a_ref, a_ref).real *
                                                                        np.vdot(a_tc, a_tc).real))}
+        elif args.circuit == "qft" and args.qubits <= 33:
+            # Beside the unfused QFT (diagonal terms deferred) timed above: the
+            # middle end's fusion into blocks of up to 6 qubits (6-qubit blocks
+            # run as dense sweeps) and into blocks of up to 5 qubits (tensor
+            # cores).  Every result's sampled amplitudes are compared with the
+            # analytic QFT|0>, whose amplitudes are all 2^(-n/2).
+            from qlassical_b200 import circuits
+            from qlassical_b200.middleware import Middleware, TranspilerConfig
+            rng = np.random.default_rng(5)
+            idx = rng.integers(0, 1 << n, size=1 << 16, dtype=np.uint64)
+            exact = 1.0 / math.sqrt(float(1 << n))
+
+            def max_err():
+                return float(np.max(np.abs(eng.amplitudes_at(idx) - exact)))
+
+            eng.set_mode(args.mode)
+            eng.reset()
+            eng.run(plan)
+            check = {"vs": "analytic QFT|0> (every amplitude 2^(-n/2))", "sampled_amplitudes": int(idx.size),
+                     "max_abs_diff": max_err()}
+            for k, key in ((5, "fused_k5_tensor_cores"), (6, "fused_k6")):
+                fm = Middleware().transpile(circuits.qft(n), config=TranspilerConfig(max_fusion_qubits=k))
+                fms, fst = one_run(fm, "tiled_tc")
+                comparisons[key] = {"value": amp_updates_step / (fms / 1e3), "ms": fms,
+                                    "tile_passes": fst["tile_passes"], "sweeps": fst["sweeps"],
+                                    "max_abs_diff_vs_analytic": max_err()}
         eng.set_mode(args.mode)
 
     line = {
