@@ -860,7 +860,7 @@ private:
             break;
         case TOP_SWAP:
             op.code = static_cast<uint16_t>(OPC_SWAP + reg_pair_index(r0, static_cast<uint32_t>(h.r1)));
-            pass_features_ |= kPassWide;
+            pass_features_ |= kPassSwaps;
             break;
         case TOP_CPHASE:
             op.code = OPC_CPHASE;

@@ -691,9 +691,15 @@ __device__ __forceinline__ void op_cphase(float2 (&v)[NR], uint32_t cm, float2 p
         if ((static_cast<uint32_t>(i) & cm) == cm) v[i] = cmul(v[i], p);
 }
 
+// Kernel instantiations by code body: 1-qubit, controlled and diagonal ops
+// (kLevelNarrow); those plus register SWAPs (kLevelSwaps); everything,
+// including the multi-qubit and tensor-core ops (kLevelWide).  A pass runs the
+// smallest that holds its ops: the larger bodies cost instruction-fetch stalls.
+constexpr int kLevelNarrow = 0, kLevelSwaps = 1, kLevelWide = 2;
+
 // The op loop of one phase.  Each op is four 16-byte words; the first holds
 // the dispatch code, the register controls and the data offset.
-template <bool WIDE>
+template <int LEVEL>
 __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, const TileOp* ops,
                                         const float2* __restrict__ mats, float2* sm, const PhaseMap& M,
                                         bool linear, TcCtx& tc, uint32_t skip = 0) {
@@ -736,6 +742,17 @@ __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, co
     case OPC_X_CTL + RR:                                                                              \
         for_pairs_ctl<RR>(v, cm, [](float2& x, float2& y) { const float2 t = x; x = y; y = t; });     \
         break;
+#define QLB_SWAP_CASES                                                                                \
+    case OPC_SWAP + reg_pair_index(0, 1): op_swap<0, 1>(v, cm); break;                                \
+    case OPC_SWAP + reg_pair_index(0, 2): op_swap<0, 2>(v, cm); break;                                \
+    case OPC_SWAP + reg_pair_index(0, 3): op_swap<0, 3>(v, cm); break;                                \
+    case OPC_SWAP + reg_pair_index(0, 4): op_swap<0, 4>(v, cm); break;                                \
+    case OPC_SWAP + reg_pair_index(1, 2): op_swap<1, 2>(v, cm); break;                                \
+    case OPC_SWAP + reg_pair_index(1, 3): op_swap<1, 3>(v, cm); break;                                \
+    case OPC_SWAP + reg_pair_index(1, 4): op_swap<1, 4>(v, cm); break;                                \
+    case OPC_SWAP + reg_pair_index(2, 3): op_swap<2, 3>(v, cm); break;                                \
+    case OPC_SWAP + reg_pair_index(2, 4): op_swap<2, 4>(v, cm); break;                                \
+    case OPC_SWAP + reg_pair_index(3, 4): op_swap<3, 4>(v, cm); break;
 #define QLB_PAIR_CASES(A, B)                                                                          \
     case OPC_SWAP + reg_pair_index(A, B): op_swap<A, B>(v, cm); break;                                \
     case OPC_U2 + reg_pair_index(A, B): op_u2<A, B>(v, mats + data, cm); break;
@@ -755,9 +772,9 @@ __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, co
     case OPC_CPHASE:                                                                                  \
         op_cphase(v, cm, f2(rec[4 * oi + 2].x, rec[4 * oi + 2].y));                                  \
         break;
-        // Multi-qubit ops live only in the WIDE instantiation, so passes of
+        // Multi-qubit ops live only in the wide instantiation, so passes of
         // 1-qubit and diagonal ops run a kernel with a small code body.
-        if constexpr (WIDE) {
+        if constexpr (LEVEL == kLevelWide) {
             switch (q0.x & 0xFFFFu) {
                 QLB_COMMON_CASES
                 QLB_PAIR_CASES(0, 1) QLB_PAIR_CASES(0, 2) QLB_PAIR_CASES(0, 3) QLB_PAIR_CASES(0, 4)
@@ -799,9 +816,17 @@ __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, co
                 }
                 continue;
             }
-            switch (code) {
-                QLB_COMMON_CASES
-            default: break;
+            if constexpr (LEVEL == kLevelSwaps) {
+                switch (code) {
+                    QLB_COMMON_CASES
+                    QLB_SWAP_CASES
+                default: break;
+                }
+            } else {
+                switch (code) {
+                    QLB_COMMON_CASES
+                default: break;
+                }
             }
         }
     }
@@ -813,6 +838,7 @@ __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, co
 #undef QLB_U1_CASE
 #undef QLB_X_CASE
 #undef QLB_PAIR_CASES
+#undef QLB_SWAP_CASES
 
 // Largest i with work[i].tile_begin <= tile (entries sorted by tile_begin).
 __device__ __forceinline__ uint32_t find_work(const TileWork* __restrict__ work, uint32_t n_work, uint64_t tile) {
@@ -830,7 +856,7 @@ __device__ __forceinline__ uint32_t find_work(const TileWork* __restrict__ work,
 // state: one entry passed by value, n_work = 0).  A CTA restages the pass
 // descriptor, phases and ops in shared memory when its next tile belongs to
 // a different pass.
-template <bool WIDE>
+template <int LEVEL>
 __global__ void __launch_bounds__(NT, 1)
 k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work, uint64_t ntiles, int features,
             int* __restrict__ err) {
@@ -950,7 +976,7 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
         PhaseMap M = make_map(P, phases[0], base);
 #pragma unroll
         for (int m = 0; m < NR; ++m) v[m] = cur[local_of(M, m)];
-        bool good = run_ops<WIDE>(v, phases[0], ops, mats, cur, M, true, tc);
+        bool good = run_ops<LEVEL>(v, phases[0], ops, mats, cur, M, true, tc);
         // Transposes alternate between the transpose buffer and `cur`: the
         // buffer written at transition k was last read at transition k-2,
         // before barrier k-1, so one barrier per transition suffices.
@@ -958,14 +984,14 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
         for (uint32_t p = 1; p < nph && good; ++p) {
             float2* wbuf = (rbuf == xbuf) ? cur : xbuf;
             if (wbuf == xbuf) xbuf_free();
-            if constexpr (WIDE) {
+            if constexpr (LEVEL == kLevelWide) {
                 const TilePhase& ph = phases[p];
                 if (ph.flags & kPhaseTcEntry) {
                     const uint32_t data = reinterpret_cast<const uint4*>(ops)[4 * ph.op_begin].w;
                     good = tc_entry(v, ph, mats + data, wbuf, tc);
                     M = make_map(P, ph, base);
                     rbuf = wbuf;
-                    if (good) good = run_ops<WIDE>(v, ph, ops, mats, rbuf, M, false, tc, 1);
+                    if (good) good = run_ops<LEVEL>(v, ph, ops, mats, rbuf, M, false, tc, 1);
                     continue;
                 }
             }
@@ -976,7 +1002,7 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
 #pragma unroll
             for (int m = 0; m < NR; ++m) v[m] = wbuf[slot_of(M, m)];
             rbuf = wbuf;
-            good = run_ops<WIDE>(v, phases[p], ops, mats, rbuf, M, false, tc);
+            good = run_ops<LEVEL>(v, phases[p], ops, mats, rbuf, M, false, tc);
         }
         if (!good) {     // a tensor-core wait gave up (every thread agrees)
             if (threadIdx.x == 0) atomicExch(err, 2);
@@ -1049,10 +1075,13 @@ cudaError_t launch_wait_selftest(uint64_t limit_ns, int* err, cudaStream_t s) {
 cudaError_t configure_tile_kernel() {
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_tile_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(k_tile_pass<kLevelNarrow>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              static_cast<int>(kSmemTotal));
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_tile_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            e = cudaFuncSetAttribute(k_tile_pass<kLevelSwaps>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(kSmemTotal));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_tile_pass<kLevelWide>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(kSmemTotal));
         if (e != cudaSuccess) return e;
         configured = true;
@@ -1064,9 +1093,11 @@ namespace {
 void launch_tile_kernel(unsigned grid, const TileWork& single, const TileWork* work, uint32_t n_work, uint64_t ntiles,
                         int features, int* err, cudaStream_t s) {
     if (features & (kPassWide | kPassTensorCores))
-        k_tile_pass<true><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
+        k_tile_pass<kLevelWide><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
+    else if (features & kPassSwaps)
+        k_tile_pass<kLevelSwaps><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
     else
-        k_tile_pass<false><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
+        k_tile_pass<kLevelNarrow><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
 }
 }  // namespace
 

@@ -162,9 +162,11 @@ struct TileWork {
 };
 
 // Kernel features of a pass: tensor-core ops (the CTA allocates tensor
-// memory) and multi-qubit ops (SWAP, U2, DENSE: the larger kernel body).
+// memory), multi-qubit ops (U2, DENSE: the largest kernel body) and register
+// SWAPs (a mid-size body; a pass with both runs the largest).
 constexpr int kPassTensorCores = 1;
 constexpr int kPassWide = 2;
+constexpr int kPassSwaps = 4;
 
 // `err` (device int) receives a nonzero code if a bounded wait gave up.
 // `features`: the pass's kPass* bits (union over the entries of a work list).
