@@ -876,7 +876,7 @@ private:
             for (const cd& z : h.mat) prog.mats.push_back(f2(z));
             if (prog.mats.size() & 1) prog.mats.push_back(make_float2(0.f, 0.f));
             if (h.kind == TOP_DENSE) stats.dense_ops += 1;
-            pass_features_ |= kPassWide;
+            pass_features_ |= h.kind == TOP_U2 ? kPassPairs : kPassWide;
             break;
         }
         default: break;
@@ -936,7 +936,7 @@ private:
         prog.ops.push_back(op);
         stats.dense_ops += 1;
         stats.tc_ops += 1;
-        pass_features_ |= kPassTensorCores | kPassWide;
+        pass_features_ |= kPassTensorCores;
     }
 
     // Register-local ops waiting to be fused into one tensor-core op.

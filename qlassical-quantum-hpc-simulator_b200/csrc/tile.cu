@@ -692,10 +692,11 @@ __device__ __forceinline__ void op_cphase(float2 (&v)[NR], uint32_t cm, float2 p
 }
 
 // Kernel instantiations by code body: 1-qubit, controlled and diagonal ops
-// (kLevelNarrow); those plus register SWAPs (kLevelSwaps); everything,
-// including the multi-qubit and tensor-core ops (kLevelWide).  A pass runs the
-// smallest that holds its ops: the larger bodies cost instruction-fetch stalls.
-constexpr int kLevelNarrow = 0, kLevelSwaps = 1, kLevelWide = 2;
+// (kLevelNarrow); those plus register SWAPs (kLevelSwaps); plus the register
+// pair ops and the tensor-core ops (kLevelTc); plus the FP32 DENSE3-5
+// handlers (kLevelWide).  A pass runs the smallest that holds its ops: the
+// larger bodies cost instruction-fetch stalls.
+constexpr int kLevelNarrow = 0, kLevelSwaps = 1, kLevelTc = 2, kLevelWide = 3;
 
 // The op loop of one phase.  Each op is four 16-byte words; the first holds
 // the dispatch code, the register controls and the data offset.
@@ -783,6 +784,17 @@ __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, co
             case OPC_DENSE3: op_dense_reg<3>(v, mats + data); break;
             case OPC_DENSE4: op_dense_reg<4>(v, mats + data); break;
             case OPC_DENSE5: op_dense5(v, mats + data, sm, M, linear); break;
+            case OPC_DENSE_TC:                 // CTA-wide; never controlled
+                if (!op_dense_tc(v, mats + data, sm, tc)) return false;
+                break;
+            default: break;
+            }
+        } else if constexpr (LEVEL == kLevelTc) {
+            switch (q0.x & 0xFFFFu) {
+                QLB_COMMON_CASES
+                QLB_PAIR_CASES(0, 1) QLB_PAIR_CASES(0, 2) QLB_PAIR_CASES(0, 3) QLB_PAIR_CASES(0, 4)
+                QLB_PAIR_CASES(1, 2) QLB_PAIR_CASES(1, 3) QLB_PAIR_CASES(1, 4)
+                QLB_PAIR_CASES(2, 3) QLB_PAIR_CASES(2, 4) QLB_PAIR_CASES(3, 4)
             case OPC_DENSE_TC:                 // CTA-wide; never controlled
                 if (!op_dense_tc(v, mats + data, sm, tc)) return false;
                 break;
@@ -984,7 +996,7 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
         for (uint32_t p = 1; p < nph && good; ++p) {
             float2* wbuf = (rbuf == xbuf) ? cur : xbuf;
             if (wbuf == xbuf) xbuf_free();
-            if constexpr (LEVEL == kLevelWide) {
+            if constexpr (LEVEL >= kLevelTc) {
                 const TilePhase& ph = phases[p];
                 if (ph.flags & kPhaseTcEntry) {
                     const uint32_t data = reinterpret_cast<const uint4*>(ops)[4 * ph.op_begin].w;
@@ -1081,6 +1093,9 @@ cudaError_t configure_tile_kernel() {
             e = cudaFuncSetAttribute(k_tile_pass<kLevelSwaps>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(kSmemTotal));
         if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_tile_pass<kLevelTc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(kSmemTotal));
+        if (e == cudaSuccess)
             e = cudaFuncSetAttribute(k_tile_pass<kLevelWide>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(kSmemTotal));
         if (e != cudaSuccess) return e;
@@ -1092,8 +1107,10 @@ cudaError_t configure_tile_kernel() {
 namespace {
 void launch_tile_kernel(unsigned grid, const TileWork& single, const TileWork* work, uint32_t n_work, uint64_t ntiles,
                         int features, int* err, cudaStream_t s) {
-    if (features & (kPassWide | kPassTensorCores))
+    if (features & kPassWide)
         k_tile_pass<kLevelWide><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
+    else if (features & (kPassTensorCores | kPassPairs))
+        k_tile_pass<kLevelTc><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
     else if (features & kPassSwaps)
         k_tile_pass<kLevelSwaps><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
     else

@@ -161,12 +161,14 @@ struct TileWork {
     uint32_t pad;
 };
 
-// Kernel features of a pass: tensor-core ops (the CTA allocates tensor
-// memory), multi-qubit ops (U2, DENSE: the largest kernel body) and register
-// SWAPs (a mid-size body; a pass with both runs the largest).
+// Kernel features of a pass, which pick the kernel body it runs (the
+// smallest that holds its ops): tensor-core ops (the CTA allocates tensor
+// memory), FP32 DENSE3-5 ops (the largest body), register SWAPs and U2
+// register-pair ops.
 constexpr int kPassTensorCores = 1;
 constexpr int kPassWide = 2;
 constexpr int kPassSwaps = 4;
+constexpr int kPassPairs = 8;
 
 // `err` (device int) receives a nonzero code if a bounded wait gave up.
 // `features`: the pass's kPass* bits (union over the entries of a work list).
