@@ -844,6 +844,7 @@ private:
                 op.kind = TOP_U1;
                 op.code = static_cast<uint16_t>(OPC_U1_CTL + r0);
                 for (int i = 0; i < 4; ++i) op.m[i] = f2(h.m[i]);
+                pass_features_ |= kPassCtl;
             } else if (h.kind == TOP_U1) {
                 op.code = static_cast<uint16_t>(OPC_U1 + r0);
                 for (int i = 0; i < 4; ++i) op.m[i] = f2(h.m[i]);
@@ -857,6 +858,7 @@ private:
             break;
         case TOP_X:
             op.code = static_cast<uint16_t>((h.cm != 0 ? OPC_X_CTL : OPC_X) + r0);
+            pass_features_ |= kPassCtl;
             break;
         case TOP_SWAP:
             op.code = static_cast<uint16_t>(OPC_SWAP + reg_pair_index(r0, static_cast<uint32_t>(h.r1)));
@@ -865,6 +867,7 @@ private:
         case TOP_CPHASE:
             op.code = OPC_CPHASE;
             op.m[0] = f2(h.m[0]);
+            pass_features_ |= kPassCtl;
             break;
         case TOP_U2: case TOP_DENSE: {
             op.k = static_cast<uint8_t>(h.k);

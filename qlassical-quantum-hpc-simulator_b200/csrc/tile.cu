@@ -692,9 +692,9 @@ __device__ __forceinline__ void op_cphase(float2 (&v)[NR], uint32_t cm, float2 p
 }
 
 // Kernel instantiations by code body: 1-qubit, controlled and diagonal ops
-// (kLevelNarrow); those plus register SWAPs (kLevelSwaps); plus the register
-// pair ops and the tensor-core ops (kLevelTc); plus the FP32 DENSE3-5
-// handlers (kLevelWide).  A pass runs the smallest that holds its ops: the
+// (kLevelNarrow); those plus register SWAPs (kLevelSwaps); uncontrolled
+// 1-qubit rotations, diagonal, SWAP, U2 and tensor-core ops (kLevelTc);
+// everything, with the FP32 DENSE3-5 handlers (kLevelWide).  A pass runs the smallest that holds its ops: the
 // larger bodies cost instruction-fetch stalls.
 constexpr int kLevelNarrow = 0, kLevelSwaps = 1, kLevelTc = 2, kLevelWide = 3;
 
@@ -725,12 +725,14 @@ __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, co
         const float c = __uint_as_float(a.x), s = __uint_as_float(a.y);                               \
         for_pairs<RR>(v, [&](float2& x, float2& y) { rx_pair(x, y, c, s); });                         \
     } break;
-#define QLB_U1_CASE(RR)                                                                               \
+#define QLB_U1_NC_CASE(RR)                                                                            \
     case OPC_U1 + RR: {                                                                               \
         const uint4 a = rec[4 * oi + 2], b = rec[4 * oi + 3];                                         \
         const float2 m[4] = {f2(a.x, a.y), f2(a.z, a.w), f2(b.x, b.y), f2(b.z, b.w)};                 \
         for_pairs<RR>(v, [&](float2& x, float2& y) { u1_pair(x, y, m); });                            \
-    } break;                                                                                          \
+    } break;
+#define QLB_U1_CASE(RR)                                                                               \
+    QLB_U1_NC_CASE(RR)                                                                                \
     case OPC_U1_CTL + RR: {                                                                           \
         const uint4 a = rec[4 * oi + 2], b = rec[4 * oi + 3];                                         \
         const float2 m[4] = {f2(a.x, a.y), f2(a.z, a.w), f2(b.x, b.y), f2(b.z, b.w)};                 \
@@ -757,11 +759,7 @@ __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, co
 #define QLB_PAIR_CASES(A, B)                                                                          \
     case OPC_SWAP + reg_pair_index(A, B): op_swap<A, B>(v, cm); break;                                \
     case OPC_U2 + reg_pair_index(A, B): op_u2<A, B>(v, mats + data, cm); break;
-#define QLB_COMMON_CASES                                                                              \
-    QLB_U1R_CASE(0) QLB_U1R_CASE(1) QLB_U1R_CASE(2) QLB_U1R_CASE(3) QLB_U1R_CASE(4)                   \
-    QLB_RX_CASE(0) QLB_RX_CASE(1) QLB_RX_CASE(2) QLB_RX_CASE(3) QLB_RX_CASE(4)                        \
-    QLB_U1_CASE(0) QLB_U1_CASE(1) QLB_U1_CASE(2) QLB_U1_CASE(3) QLB_U1_CASE(4)                        \
-    QLB_X_CASE(0) QLB_X_CASE(1) QLB_X_CASE(2) QLB_X_CASE(3) QLB_X_CASE(4)                             \
+#define QLB_DIAG_CASE                                                                                 \
     case OPC_DIAG: {                                                                                  \
         const uint32_t n_words = rec[4 * oi + 2].x;    /* 0: read from global memory */              \
         const uint4 q1 = rec[4 * oi + 1];                                                             \
@@ -769,7 +767,13 @@ __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, co
         const float2* tab = staged ? diag_stage(mats + data, n_words, tc.sb) : mats + data;           \
         op_diag(v, tab, q1.x, q1.y & 0xFFFFu, q1.y >> 16, cm, M.gt);                                  \
         if (staged) __syncthreads();   /* the staging area is free again */                           \
-    } break;                                                                                          \
+    } break;
+#define QLB_COMMON_CASES                                                                              \
+    QLB_U1R_CASE(0) QLB_U1R_CASE(1) QLB_U1R_CASE(2) QLB_U1R_CASE(3) QLB_U1R_CASE(4)                   \
+    QLB_RX_CASE(0) QLB_RX_CASE(1) QLB_RX_CASE(2) QLB_RX_CASE(3) QLB_RX_CASE(4)                        \
+    QLB_U1_CASE(0) QLB_U1_CASE(1) QLB_U1_CASE(2) QLB_U1_CASE(3) QLB_U1_CASE(4)                        \
+    QLB_X_CASE(0) QLB_X_CASE(1) QLB_X_CASE(2) QLB_X_CASE(3) QLB_X_CASE(4)                             \
+    QLB_DIAG_CASE                                                                                     \
     case OPC_CPHASE:                                                                                  \
         op_cphase(v, cm, f2(rec[4 * oi + 2].x, rec[4 * oi + 2].y));                                  \
         break;
@@ -790,8 +794,12 @@ __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, co
             default: break;
             }
         } else if constexpr (LEVEL == kLevelTc) {
+            // no X, controlled 1-qubit or CPHASE handlers: passes with those run the wide body
             switch (q0.x & 0xFFFFu) {
-                QLB_COMMON_CASES
+                QLB_U1R_CASE(0) QLB_U1R_CASE(1) QLB_U1R_CASE(2) QLB_U1R_CASE(3) QLB_U1R_CASE(4)
+                QLB_RX_CASE(0) QLB_RX_CASE(1) QLB_RX_CASE(2) QLB_RX_CASE(3) QLB_RX_CASE(4)
+                QLB_U1_NC_CASE(0) QLB_U1_NC_CASE(1) QLB_U1_NC_CASE(2) QLB_U1_NC_CASE(3) QLB_U1_NC_CASE(4)
+                QLB_DIAG_CASE
                 QLB_PAIR_CASES(0, 1) QLB_PAIR_CASES(0, 2) QLB_PAIR_CASES(0, 3) QLB_PAIR_CASES(0, 4)
                 QLB_PAIR_CASES(1, 2) QLB_PAIR_CASES(1, 3) QLB_PAIR_CASES(1, 4)
                 QLB_PAIR_CASES(2, 3) QLB_PAIR_CASES(2, 4) QLB_PAIR_CASES(3, 4)
@@ -848,6 +856,8 @@ __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, co
 #undef QLB_U1R_CASE
 #undef QLB_RX_CASE
 #undef QLB_U1_CASE
+#undef QLB_U1_NC_CASE
+#undef QLB_DIAG_CASE
 #undef QLB_X_CASE
 #undef QLB_PAIR_CASES
 #undef QLB_SWAP_CASES
@@ -1108,6 +1118,8 @@ namespace {
 void launch_tile_kernel(unsigned grid, const TileWork& single, const TileWork* work, uint32_t n_work, uint64_t ntiles,
                         int features, int* err, cudaStream_t s) {
     if (features & kPassWide)
+        k_tile_pass<kLevelWide><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
+    else if ((features & (kPassTensorCores | kPassPairs)) && (features & kPassCtl))
         k_tile_pass<kLevelWide><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
     else if (features & (kPassTensorCores | kPassPairs))
         k_tile_pass<kLevelTc><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);

@@ -134,7 +134,7 @@ struct TilePass {
     uint8_t tile_pos[kTileQubits];    // tile-local position j -> memory qubit (ascending)
     uint8_t n_out;                    // number of non-tile qubits
     uint8_t n_low;                    // tile_pos[j] == j for j < n_low (>= kTileLow): runs of 2^n_low amps
-    uint8_t has_tc;                   // kernel features the pass needs (kPassTensorCores | kPassWide)
+    uint8_t has_tc;                   // kernel features the pass needs (kPass* bits)
     uint8_t out_mem[40];              // non-tile memory qubits, ascending
     uint32_t phase_begin, phase_end;
 };
@@ -163,12 +163,14 @@ struct TileWork {
 
 // Kernel features of a pass, which pick the kernel body it runs (the
 // smallest that holds its ops): tensor-core ops (the CTA allocates tensor
-// memory), FP32 DENSE3-5 ops (the largest body), register SWAPs and U2
-// register-pair ops.
+// memory), FP32 DENSE3-5 ops (the largest body), register SWAPs, U2
+// register-pair ops, and X, controlled 1-qubit and CPHASE ops (not in the
+// tensor-core body).
 constexpr int kPassTensorCores = 1;
 constexpr int kPassWide = 2;
 constexpr int kPassSwaps = 4;
 constexpr int kPassPairs = 8;
+constexpr int kPassCtl = 16;
 
 // `err` (device int) receives a nonzero code if a bounded wait gave up.
 // `features`: the pass's kPass* bits (union over the entries of a work list).
