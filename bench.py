@@ -43,10 +43,10 @@ UNIT = "amp-updates/s"
 
 # DRAM bytes (read + write) of one tile pass per algorithmic byte (16 B per
 # amplitude), from one ncu capture of a 26-qubit tensor-core pass of the
-# fused circuit (profiles/k_tile_pass_tensorcore_fused_26q_depth8.md: 1014.4 MB
+# fused circuit (profiles/k_tile_pass_tensorcore_fused_26q_depth8.md: 1014.7 MB
 # over 1073.7 MB); a pass's traffic grows in proportion to the amplitudes it
 # processes, so full-size launches are scaled by this ratio.
-TRAFFIC_PER_ALGORITHMIC_BYTE = 1014.4 / 1073.7
+TRAFFIC_PER_ALGORITHMIC_BYTE = 1014.7 / 1073.7
 
 
 def parse():
