@@ -42,10 +42,10 @@ METRIC = "amp-updates/s"
 UNIT = "amp-updates/s"
 
 # DRAM bytes (read + write) of one tile pass per algorithmic byte (16 B per
-# amplitude), from one ncu capture of a 26-qubit tensor-core pass of the
-# fused circuit (profiles/k_tile_pass_tensorcore_fused_26q_depth8.md: 1014.7 MB
-# over 1073.7 MB); a pass's traffic grows in proportion to the amplitudes it
-# processes, so full-size launches are scaled by this ratio.
+# amplitude): ncu's dram__bytes_read.sum + dram__bytes_write.sum of one
+# tensor-core pass of the fused rotation circuit at 26 qubits, 1014.7 MB
+# against 1073.7 MB algorithmic.  A pass's traffic grows in proportion to
+# the amplitudes it processes, so full-size launches are scaled by this ratio.
 TRAFFIC_PER_ALGORITHMIC_BYTE = 1014.7 / 1073.7
 
 
@@ -99,11 +99,8 @@ def logical_gates(args, module):
 
 
 def config_of(args, module, extra=None):
-    name = (f"QFT (H + CP ladders + bit-reversal swaps), {args.qubits} qubits" if args.circuit == "qft" else
-            f"random RX/RY/RZ + CZ-pairs circuit, {args.qubits} qubits, depth {args.depth}"
-            + (", middle-end fusion k<=5 + windowing" if args.circuit == "fused" else ""))
     c = {
-        "workload": name,
+        "workload": _workload_name(args),
         "n_qubits": args.qubits,
         "depth": args.depth,
         "seed": args.seed,
@@ -166,71 +163,125 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def reference_sample(module, gates):
-    """The first `gates` instructions of the circuit in the reference's IR
-    (CZ / CP as 2-qubit UNITARY diagonals), transpiled by the reference's own
-    middle end with its best valid setting (fusion k <= 4, windowing off).
-    Transpiling is not timed, as in the reference's benchmark loop
-    (bench_hw_awareness.cpp:85-107)."""
-    from oracle import oracle
-    from qlassical_b200 import circuits
-    from qlassical_b200.ir import IRModule, UnitaryPool
-    ref = circuits.to_reference_ir(module)
-    sample = IRModule(module.num_qubits, unitary_pool=ref.unitaries())
-    sample.set_program(ref.program()[:gates])
-    prog, data, meta = oracle.transpile_reference(sample, fusion=True, hw=False)
-    fused = IRModule(module.num_qubits, unitary_pool=UnitaryPool.from_arrays(data, meta))
-    fused.set_program(prog)
-    return fused
+def reference_circuit(args):
+    """The workload in the reference's own IR, built by numpy alone
+    (oracle/ref_workloads.py: no import of the package under test).  The
+    reference engine applies dense blocks of at most 4 qubits
+    (cpu_openmp_engine.hpp:539-606), so it gets the unfused circuit and
+    fuses it with its own middle end."""
+    from oracle import ref_workloads
+    if args.circuit == "qft":
+        return ref_workloads.qft(min(args.qubits, REF_MAX_QUBITS))
+    return ref_workloads.random_rot_cz(min(args.qubits, REF_MAX_QUBITS), args.depth, seed=args.seed)
 
 
-def cpu_baseline(args, module, max_gates):
-    """The reference CPUOpenMPEngine (oracle/_ref, its Release flags) on the
-    first `max_gates` logical gates of the same circuit at the same size."""
+# complex128 on the host: 30 qubits = 17.2 GB; larger states are timed at 30.
+REF_MAX_QUBITS = 30
+
+
+def reference_layer_samples(rc, layers):
+    """Whole layers of the circuit (rotations on every qubit plus that
+    layer's CZ diagonals), each transpiled by the reference's own middle end
+    with its best valid setting (fusion k <= 4, windowing off) -- untimed, as
+    in the reference's benchmark loop (bench_hw_awareness.cpp:85-107)."""
+    from oracle import oracle, ref_workloads
+    out = []
+    for layer in layers:
+        one = rc.layers(layer, 1)
+        prog, data, meta = oracle.transpile_reference(one, fusion=True, hw=False)
+        out.append((one.gate_count(), ref_workloads.RefCircuit(rc.num_qubits, prog, data, meta)))
+    return out
+
+
+def cpu_baseline(args):
+    """The reference CPUOpenMPEngine (oracle/_ref, its Release flags, all
+    host threads) on one whole layer of the same circuit at the same size."""
     from oracle import oracle
-    sample = reference_sample(module, max_gates)
-    t = oracle.time_reference(sample, reps=1)
-    value = max_gates * float(1 << module.num_qubits) / t
+    rc = reference_circuit(args)
+    if args.circuit == "qft":
+        prog, data, meta = oracle.transpile_reference(rc, fusion=True, hw=False)
+        from oracle import ref_workloads
+        sample = [(rc.gate_count(), ref_workloads.RefCircuit(rc.num_qubits, prog, data, meta))]
+    else:
+        sample = reference_layer_samples(rc, [0])
+    gates, fused = sample[0]
+    t = oracle.time_reference(fused, reps=1)
+    value = gates * float(1 << rc.num_qubits) / t
+    what = "the whole QFT" if args.circuit == "qft" else "layer 0 (rotations on every qubit + its CZ diagonals)"
     return {"value": value, "unit": UNIT, "cores": oracle.reference_threads(), "kind": "reference",
-            "sample": f"first {max_gates} of {module.gate_count()} gates of the same {module.num_qubits}-qubit "
-                      f"circuit, reference fusion k<=4 ({sample.gate_count()} instructions), complex128, {t:.2f} s"}
+            "sample": f"{what}, {gates} gates of the same {rc.num_qubits}-qubit circuit, reference fusion k<=4 "
+                      f"({fused.gate_count()} instructions), complex128, {t:.2f} s"}
 
 
 def run_reference(args):
+    """The reference arm: the unmodified reference CPUOpenMPEngine (compiled
+    from its own headers into oracle/_ref) through its stock execute() on
+    the box's host cores.  Each step times one whole layer of the benchmark
+    circuit (step s: layer s mod depth), so the steps together sample the
+    full circuit; value = logical amp-updates per second over the timed
+    layers, the rate the whole circuit would run at."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     os.environ.setdefault("OMP_PROC_BIND", "true")
     os.environ.setdefault("OMP_PLACES", "cores")
-    from __graft_entry__ import package
-    package()   # the circuit generators and IR types (no GPU work on this arm)
-    # The reference engine applies blocks of at most 4 qubits
-    # (cpu_openmp_engine.hpp:539-606): it gets the unfused circuit and fuses
-    # it with its own middle end.
-    module = workload(args) if args.circuit != "fused" else circuits_rot_cz(args)
     from oracle import oracle
     if not oracle.reference_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference sources absent)"}))
         return
-    gates = 30
-    sample = reference_sample(module, gates)
-    for _ in range(args.warmup):
-        oracle.time_reference(sample, reps=1)
-    times = [oracle.time_reference(sample, reps=1) for _ in range(args.steps)]
+    if args.workload != "circuit":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched or serving mode; "
+                                                              "its engine is timed on the circuit workloads"}))
+        return
+    rc = reference_circuit(args)
+    n = rc.num_qubits
+    if args.circuit == "qft":
+        prog, data, meta = oracle.transpile_reference(rc, fusion=True, hw=False)
+        from oracle import ref_workloads
+        samples = [(rc.gate_count(), ref_workloads.RefCircuit(n, prog, data, meta))]
+        desc = "the whole QFT per step"
+    else:
+        samples = reference_layer_samples(rc, range(args.depth))
+        desc = "one whole layer per step (layer s mod depth: rotations on every qubit + that layer's CZ diagonals)"
+    for w in range(args.warmup):
+        oracle.time_reference(samples[w % len(samples)][1], reps=1)
+    times, gates = [], 0
+    for s_ in range(args.steps):
+        g, fused = samples[s_ % len(samples)]
+        times.append(oracle.time_reference(fused, reps=1))
+        gates += g
     total = sum(times)
-    value = args.steps * gates * float(1 << module.num_qubits) / total
+    value = gates * float(1 << n) / total
     cores = oracle.reference_threads()
+    full_gates = rc.gate_count()
+    cfg = {
+        "workload": _workload_name(args),
+        "n_qubits": n, "depth": args.depth, "seed": args.seed,
+        "sample": desc,
+        "sample_gates_per_step": gates / args.steps,
+        "full_circuit_gates": full_gates,
+        "full_circuit_seconds_extrapolated": full_gates * float(1 << n) / value,
+        "fusion": "reference middle end, fusion k<=4, windowing off (its best valid setting)",
+    }
+    if args.qubits > n:
+        cfg["size_limit"] = f"timed at {n} qubits: a complex128 state of {args.qubits} qubits does not fit host RAM"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
-        "data": "synthetic", "config": config_of(args, module, {"sample_gates_per_step": gates}),
+        "data": "synthetic", "config": cfg,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": f"first {gates} gates of the circuit per step, reference fusion k<=4 "
-                                   f"({sample.gate_count()} instructions), complex128, CPUOpenMPEngine"},
+                         "sample": f"{desc}; CPUOpenMPEngine, complex128, {cores} threads"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+
+
+def _workload_name(args):
+    if args.circuit == "qft":
+        return f"QFT (H + CP ladders + bit-reversal swaps), {args.qubits} qubits"
+    return (f"random RX/RY/RZ + CZ-pairs circuit, {args.qubits} qubits, depth {args.depth}"
+            + (", middle-end fusion k<=5 + windowing" if args.circuit == "fused" else ""))
 
 
 def run_ours(args):
@@ -348,26 +399,42 @@ def run_ours(args):
         pms, pst = one_run(module, "plain")
         plain = {"value": amp_updates_step / (pms / 1e3), "ms": pms, "sweeps": pst["sweeps"],
                  "kind": "one sweep per instruction (same circuit)"}
-        if args.circuit == "fused":
-            # the same fused blocks on FP32 CUDA cores, then the unfused circuit
-            # through the CUDA-core tile path; the last state is the reference
-            # for a sampled accuracy check of the tensor-core result
-            fms, _ = one_run(module, "tiled")
-            comparisons["fp32_fused"] = {"value": amp_updates_step / (fms / 1e3), "ms": fms}
-            rng = np.random.default_rng(5)
-            idx = rng.integers(0, 1 << n, size=1 << 16, dtype=np.uint64)
-            eng.set_mode(args.mode)
-            eng.reset()
-            eng.run(plan)
-            a_tc = eng.amplitudes_at(idx)
-            ums, _ = one_run(circuits_rot_cz(args), "tiled")
-            a_ref = eng.amplitudes_at(idx)
-            comparisons["unfused_fp32_tiles"] = {"value": amp_updates_step / (ums / 1e3), "ms": ums}
-            ip = np.vdot(a_ref, a_tc)
-            check = {"vs": "unfused circuit on the FP32 CUDA-core tile path", "sampled_amplitudes": int(idx.size),
-                     "max_abs_diff": float(np.max(np.abs(a_tc - a_ref))),
-                     "sampled_infidelity": float(1.0 - abs(ip) ** 2 / (np.vdot(a_ref, a_ref).real *
-                                                                       np.vdot(a_tc, a_tc).real))}
+        if args.circuit in ("fused", "rot_cz") and n <= 31:
+            # Accuracy against FP64: the FP64 checker's complex128 state of the
+            # *unfused* circuit (run gate by gate in double on the device) is
+            # compared over the whole state with each complex64 result.
+            t0 = time.perf_counter()
+            chk = q.Check64(n)
+            chk.execute(circuits_rot_cz(args))
+            check_s = time.perf_counter() - t0
+            results = {}
+            if args.circuit == "fused":
+                # the same fused blocks on FP32 CUDA cores
+                fms, _ = one_run(module, "tiled")
+                comparisons["fp32_fused"] = {"value": amp_updates_step / (fms / 1e3), "ms": fms}
+                results["fp32_fused"] = chk.compare(eng)
+                # the benchmarked tensor-core run
+                eng.set_mode(args.mode)
+                eng.reset()
+                eng.run(plan)
+                results["tensor_core_fused"] = chk.compare(eng)
+                # the unfused circuit through the CUDA-core tile path
+                ums, _ = one_run(circuits_rot_cz(args), "tiled")
+                comparisons["unfused_fp32_tiles"] = {"value": amp_updates_step / (ums / 1e3), "ms": ums}
+                results["unfused_fp32_tiles"] = chk.compare(eng)
+            else:
+                eng.set_mode(args.mode)
+                eng.reset()
+                eng.run(plan)
+                results[args.mode] = chk.compare(eng)
+            chk.close()
+            check = {"vs": "FP64 checker: the unfused circuit in complex128 on the device, gate by gate "
+                           "(whole-state max |delta amplitude| and infidelity, reduced in FP64)",
+                     "checker_s": check_s, "tolerance": {"infidelity": 1e-6}}
+            for key, r in results.items():
+                check[key] = {"max_abs_diff": r["max_abs_diff"], "infidelity": r["infidelity"]}
+            check["max_abs_diff"] = max(r["max_abs_diff"] for r in results.values())
+            check["infidelity"] = max(r["infidelity"] for r in results.values())
         elif args.circuit == "qft" and args.qubits <= 33:
             # Beside the unfused QFT (diagonal terms deferred) timed above: the
             # middle end's fusion into blocks of up to 6 qubits (6-qubit blocks
@@ -386,8 +453,11 @@ def run_ours(args):
             eng.set_mode(args.mode)
             eng.reset()
             eng.run(plan)
+            got = eng.amplitudes_at(idx)
             check = {"vs": "analytic QFT|0> (every amplitude 2^(-n/2))", "sampled_amplitudes": int(idx.size),
-                     "max_abs_diff": max_err()}
+                     "max_abs_diff": float(np.max(np.abs(got - exact))),
+                     "sampled_infidelity": float(1.0 - abs(np.sum(got) * exact) ** 2 /
+                                                 (idx.size * exact * exact * np.vdot(got, got).real))}
             for k, key in ((5, "fused_k5_tensor_cores"), (6, "fused_k6")):
                 fm = Middleware().transpile(circuits.qft(n), config=TranspilerConfig(max_fusion_qubits=k))
                 fms, fst = one_run(fm, "tiled_tc")
@@ -419,9 +489,7 @@ def run_ours(args):
         line["accuracy_check"] = check
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            # the reference engine takes blocks of <= 4 qubits: it runs the unfused circuit
-            base = module if args.circuit != "fused" else circuits_rot_cz(args)
-            line["cpu_baseline"] = cpu_baseline(args, base, max_gates=45)
+            line["cpu_baseline"] = cpu_baseline(args)
         except Exception as ex:  # the oracle libraries are test infrastructure
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
                                     "sample": f"unavailable: {ex}"}

@@ -211,6 +211,30 @@ int qlb_describe_plan(uint32_t num_qubits, int mode, int physical_global_swap,
 int qlb_engine_norm_sq(qlb_engine_t e, double* out);
 int qlb_engine_prob_one(qlb_engine_t e, uint32_t qubit, double* out);
 int qlb_engine_expect_z(qlb_engine_t e, double* out, uint32_t num_qubits);
+/* FP64 checker (no counterpart in the reference engine, whose arithmetic is
+ * complex128 on the host, cpu_openmp_engine.hpp:143-225): a complex128
+ * state on the device that runs a program gate by gate in double precision,
+ * for measuring the complex64 engine's error at sizes a host complex128 run
+ * cannot reach in reasonable time (30 qubits: 17.2 GB).  It accepts every
+ * instruction type except MEASURE; GLOBAL_SWAP permutes physical qubits and
+ * the state stays in logical order, as the engine's does.
+ * qlb_check64_compare() reduces, over the whole state and in FP64, the
+ * difference between the checker's state and a complex64 device state of
+ * the same size (e.g. qlb_engine_device_state()). */
+typedef struct qlb_check64* qlb_check64_t;
+typedef struct qlb_check64_result {
+    double max_abs_diff;   /* max_i |ref_i - psi_i| */
+    double infidelity;     /* 1 - |<ref|psi>|^2 / (<ref|ref> <psi|psi>) */
+    double norm_ref, norm_state;
+    double overlap_re, overlap_im;   /* <ref|psi> */
+} qlb_check64_result;
+int qlb_check64_create(qlb_check64_t* out, uint32_t num_qubits);          /* |0...0>, 1..33 qubits */
+int qlb_check64_execute(qlb_check64_t c, const qlb_gate_instr* program, uint64_t count,
+                        const qlb_pool_view* pool);
+int qlb_check64_compare(qlb_check64_t c, const void* state_float2, qlb_check64_result* out);
+int qlb_check64_download(qlb_check64_t c, double* out_c128, uint64_t dim);
+int qlb_check64_destroy(qlb_check64_t c);
+
 /* <Z_q> for every qubit of a complex64 device state, allocating nothing.
  * No counterpart in the reference.  For callers that must not allocate
  * device memory while they run -- such as a serving loop that admits
@@ -223,8 +247,10 @@ int qlb_engine_expect_z(qlb_engine_t e, double* out, uint32_t num_qubits);
  * num_qubits doubles; the call runs on `cuda_stream` and waits for it.
  * All calls share the scratch: calls whose kernels overlap on the GPU race,
  * so serialize them.  The first call on a device looks up the scratch's
- * device address with that device current; make it before any stream
- * capture starts. */
+ * device address with that device current, which is also when the device
+ * commits the scratch (the library's modules load lazily): make that first
+ * call -- a warm-up on any small state -- before any stream capture starts
+ * and before measuring the free memory to be budgeted. */
 int qlb_expect_z_noalloc(const void* state_float2, uint32_t num_qubits, double* out, void* cuda_stream);
 /* Draws `shots` basis states from |amp|^2 with a counter-based generator
  * keyed by `seed`; identical seeds give identical samples on any launch. */

@@ -20,7 +20,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libqlref.so")
 REF_EXACT_SO = os.path.join(HERE, "_ref", "libqlref_exact.so")
-REFERENCE_DIR = "/root/reference"
+# The reference source tree: $QLB_REFERENCE_DIR, else a directory named
+# `reference` beside the repository (the layout this project is built in).
+REFERENCE_DIR = os.environ.get(
+    "QLB_REFERENCE_DIR", os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 
 
 class _PoolView(ctypes.Structure):
@@ -36,7 +39,7 @@ def build(reference: bool | None = None) -> None:
         reference = os.path.isdir(os.path.join(REFERENCE_DIR, "include"))
     if reference:
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={REFERENCE_DIR}"] + targets, check=True)
 
 
 _libs: dict = {}
@@ -64,6 +67,11 @@ def _pool_args(pool_data, pool_meta):
 
 
 def _unpack_module(module):
+    """(n, program, pool data, pool metadata) of an IR module, or of a
+    ref_workloads.RefCircuit (numpy arrays only)."""
+    if hasattr(module, "arrays"):
+        n, prog, data, meta = module.arrays()
+        return n, np.ascontiguousarray(prog), data, meta
     prog = np.ascontiguousarray(module.program())
     pool = module.unitaries()
     return module.num_qubits, prog, pool.data, pool.metadata()
@@ -153,9 +161,10 @@ def transpile_reference(module, fusion=True, hw=False, cost_model=0, numa_penalt
     cnt = L.qlref_module_count(h)
     ne = L.qlref_module_pool_elements(h)
     nm = L.qlref_module_pool_matrices(h)
+    from . import ref_workloads
     out = np.zeros(cnt, dtype=prog.dtype)
     data = np.zeros(ne, dtype=np.complex128)
-    meta = np.zeros(nm, dtype=pmeta.dtype)
+    meta = np.zeros(nm, dtype=pmeta.dtype if pmeta is not None else ref_workloads.MATRIX_ENTRY_DTYPE)
     L.qlref_module_copy(h, out.ctypes.data if cnt else None, data.ctypes.data if ne else None,
                         meta.ctypes.data if nm else None)
     L.qlref_module_free(h)

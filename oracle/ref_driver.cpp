@@ -20,12 +20,20 @@
 #include <frontend/frontend.hpp>
 #include <middleware/middleware.hpp>
 
-#include "../include/qlassical_b200.h"
-
 using namespace qlassical;
 
-static_assert(sizeof(qlb_gate_instr) == sizeof(GateInstr), "GateInstr layout");
-static_assert(sizeof(qlb_matrix_entry) == sizeof(UnitaryPool::MatrixEntry), "MatrixEntry layout");
+// The ctypes side passes the reference's own GateInstr records and a plain
+// view of a UnitaryPool (complex128 data + MatrixEntry records).
+using qlb_gate_instr = GateInstr;
+using qlb_matrix_entry = UnitaryPool::MatrixEntry;
+struct qlb_pool_view {
+    const double* data;
+    uint64_t num_elements;
+    const qlb_matrix_entry* metadata;
+    uint64_t num_matrices;
+};
+static_assert(sizeof(GateInstr) == 16, "GateInstr layout");
+static_assert(sizeof(UnitaryPool::MatrixEntry) == 12, "MatrixEntry layout");
 
 namespace {
 

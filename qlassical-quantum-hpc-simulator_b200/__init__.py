@@ -8,11 +8,11 @@ include/qlassical_b200/.
 from . import _lib
 from ._lib import QlbError, lib
 from .ir import GateType, IRModule, QuantumCircuit, UnitaryPool, make_instr
-from .engine import CUDAEngine, CUDAStateVector
+from .engine import Check64, CUDAEngine, CUDAStateVector
 
 lib()  # fail loudly at import if the native library is missing
 
 __all__ = [
     "GateType", "IRModule", "QuantumCircuit", "UnitaryPool", "make_instr",
-    "CUDAEngine", "CUDAStateVector", "QlbError", "lib",
+    "CUDAEngine", "CUDAStateVector", "Check64", "QlbError", "lib",
 ]

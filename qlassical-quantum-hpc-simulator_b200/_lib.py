@@ -121,6 +121,15 @@ class RequestInfo(ctypes.Structure):
     ]
 
 
+class Check64Result(ctypes.Structure):
+    _fields_ = [("max_abs_diff", ctypes.c_double), ("infidelity", ctypes.c_double),
+                ("norm_ref", ctypes.c_double), ("norm_state", ctypes.c_double),
+                ("overlap_re", ctypes.c_double), ("overlap_im", ctypes.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class TranspileConfig(ctypes.Structure):
     _fields_ = [
         ("enable_gate_fusion", ctypes.c_int),
@@ -186,6 +195,11 @@ _SIGNATURES = {
     "qlb_engine_run": [_P, _P],
     "qlb_plan_stats": [_P, ctypes.POINTER(ExecStats)],
     "qlb_plan_destroy": [_P],
+    "qlb_check64_create": [ctypes.POINTER(_P), _U32],
+    "qlb_check64_execute": [_P, _P, _U64, ctypes.POINTER(PoolView)],
+    "qlb_check64_compare": [_P, _P, ctypes.POINTER(Check64Result)],
+    "qlb_check64_download": [_P, _P, _U64],
+    "qlb_check64_destroy": [_P],
     "qlb_batch_create": [ctypes.POINTER(_P), _U32, _P, _P, _P, _P, _I],
     "qlb_batch_run": [_P],
     "qlb_batch_synchronize": [_P],

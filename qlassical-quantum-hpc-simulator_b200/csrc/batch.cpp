@@ -35,7 +35,7 @@ struct BatchRound {
     size_t work_off;     // byte offset of its TileWork entries
     uint32_t n_work;
     uint64_t tiles;
-    int has_tc;
+    int features;
 };
 
 // One mode's device program and graph over the shared state buffer.
@@ -152,7 +152,7 @@ std::unique_ptr<BatchProgram> build_program(qlb_batch& b, int mode, const qlb_ga
             work.back().pad = c;
             R.tiles += uint64_t{1} << (b.states[c].eff_qubits - kTileQubits);
             R.n_work += 1;
-            R.has_tc |= all.passes[pid].has_tc;
+            R.features |= all.passes[pid].features;
         }
         P->tiles += R.tiles;
         P->rounds.push_back(R);
@@ -198,7 +198,7 @@ void capture(qlb_batch& b, BatchProgram& P) {
     if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), s);
     for (const BatchRound& R : P.rounds) {
         if (e != cudaSuccess) break;
-        e = launch_tile_work(reinterpret_cast<const TileWork*>(d + R.work_off), R.n_work, R.tiles, R.has_tc, err, s);
+        e = launch_tile_work(reinterpret_cast<const TileWork*>(d + R.work_off), R.n_work, R.tiles, R.features, err, s);
     }
     if (e == cudaSuccess)
         e = launch_batch_expect_z(base, st, b.count, chunks, b.chunk_begin.back(), static_cast<double*>(b.partial.p),

@@ -18,6 +18,7 @@
 #include "engine.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -32,18 +33,18 @@ namespace qlb {
 namespace {
 thread_local std::string g_last_error;
 
-int& cached_sm_count() {
-    static int v = 0;
-    return v;
-}
+// Multiprocessor count per device index, looked up on first use.
+constexpr int kMaxDevices = 64;
+std::atomic<int> g_sm_count[kMaxDevices];
 }  // namespace
 
 int sm_count() {
-    int& v = cached_sm_count();
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 148;
+    int v = g_sm_count[dev].load(std::memory_order_relaxed);
     if (v == 0) {
-        int dev = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
-            v = 148;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+        g_sm_count[dev].store(v, std::memory_order_relaxed);
     }
     return v;
 }
@@ -364,7 +365,6 @@ const char* qlb_version(void) { return "qlassical_b200 0.1 (sm_100a)"; }
 int qlb_set_device(int device) {
     return guarded([&] {
         check_cuda(cudaSetDevice(device), "cudaSetDevice");
-        cached_sm_count() = 0;
     });
 }
 

@@ -51,6 +51,10 @@ void state_free(qlb_state& sv);
 void state_upload_c128(qlb_state& sv, const double* amps, uint64_t dim, cudaStream_t s, DeviceBuffer& staging);
 void state_download_c128(const qlb_state& sv, double* out, cudaStream_t s, DeviceBuffer& staging);
 
+// Validates one instruction against the state size and pool; returns its
+// arity (throws QLB_ERR_UNKNOWN_GATE / QLB_ERR_INVALID_ARG).
+uint32_t validate_instr(const qlb_gate_instr& in, uint32_t n, const qlb_pool_view* pool);
+
 struct TilePlanner;  // tile.cpp
 
 }  // namespace qlb

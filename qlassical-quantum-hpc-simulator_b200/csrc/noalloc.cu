@@ -12,14 +12,19 @@
 //
 // Limits and rules (also stated in include/qlassical_b200.h):
 //   - the scratch holds kNoAllocScratchDoubles doubles (about 176 KiB) on
-//     every GPU that loads the library, for as long as the library is loaded;
+//     every GPU where the entry point has been called, from its first call
+//     (the library's modules load lazily, so the array is committed when the
+//     first call looks up its address) until the library is unloaded: a
+//     caller that budgets free memory makes a warm-up call first;
 //   - states of 1..34 qubits are accepted, anything else is rejected;
 //   - all calls share the one array, so two calls whose kernels overlap on
 //     the GPU (different streams, or host threads) race and corrupt each
 //     other's result; serialize them;
 //   - the first call on each device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture begins;
+//     before any stream capture begins.  The address is cached for the life
+//     of the process: after a cudaDeviceReset of that device it is stale, so
+//     a process that resets a device must not call this entry point again;
 //   - nothing in the scratch needs to start at zero: every partial slot the
 //     reduction reads is written by the same call first.
 #include <cstring>

@@ -20,7 +20,7 @@ enum StepKind : uint8_t {
 
 struct PlanStep {
     uint8_t kind;
-    uint8_t has_tc;     // STEP_PASS: the pass uses tensor-core ops
+    uint8_t features;   // STEP_PASS: the pass's kPass* bits (which kernel body it runs)
     uint32_t index;
     qlb_gate_instr instr;
     uint64_t mat_off;   // float2 offset of a dense matrix in the plan's device buffer

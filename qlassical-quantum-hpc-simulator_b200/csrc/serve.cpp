@@ -249,7 +249,7 @@ void serve_loop(qlb_server* sp, int lane) {
                 w.pass = st.index;
                 work[nw++] = w;
                 tiles += uint64_t{1} << (r->neff - kTileQubits);
-                features |= st.has_tc;
+                features |= st.features;
             }
             if (r->next_pass + 1 >= np) {          // finishes this round
                 bst[nfin] = BatchState{static_cast<uint64_t>((r->block_off + r->o_state) / sizeof(float2)), r->n,

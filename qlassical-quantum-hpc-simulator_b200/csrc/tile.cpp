@@ -642,10 +642,18 @@ private:
         P.phase_end = static_cast<uint32_t>(prog.phases.size());
         P.n_low = 0;
         while (P.n_low < kTileQubits && P.tile_pos[P.n_low] == P.n_low) ++P.n_low;
-        P.has_tc = static_cast<uint8_t>(pass_features_);
+        P.features = static_cast<uint8_t>(pass_features_);
+        // Every op must have a handler in the body the pass will run (a
+        // missing one would be skipped by the kernel's dispatch).
+        const int body = tile_body(pass_features_);
+        for (uint32_t pi = P.phase_begin; pi < P.phase_end; ++pi)
+            for (uint32_t oi = prog.phases[pi].op_begin; oi < prog.phases[pi].op_end; ++oi)
+                if (!tile_body_handles(body, prog.ops[oi].code))
+                    fail(QLB_ERR_CUDA, "tile planner: op code " + std::to_string(prog.ops[oi].code) +
+                                           " has no handler in kernel body " + std::to_string(body));
         PlanStep st{};
         st.kind = STEP_PASS;
-        st.has_tc = P.has_tc;
+        st.features = P.features;
         pass_features_ = 0;
         st.index = static_cast<uint32_t>(prog.passes.size());
         steps.push_back(st);
@@ -1437,8 +1445,8 @@ std::string describe_plan_json(const PlanConfig& cfg, const qlb_gate_instr* prog
         }
         out += "],\"n_low\":";
         u(P.n_low);
-        out += ",\"has_tc\":";
-        u(P.has_tc);
+        out += ",\"features\":";
+        u(P.features);
         out += ",\"phases\":[";
         for (uint32_t ph = P.phase_begin; ph < P.phase_end; ++ph) {
             const TilePhase& T = pl.prog.phases[ph];
@@ -1543,7 +1551,7 @@ void run_plan(qlb_engine& e, const qlb_plan& p) {
             check_cuda(launch_tile_pass(e.sv.d, e.sv.n, reinterpret_cast<const TilePass*>(d + p.o_pass),
                                         reinterpret_cast<const TilePhase*>(d + p.o_phase),
                                         reinterpret_cast<const TileOp*>(d + p.o_ops), mats, st.index,
-                                        static_cast<int>(st.has_tc), static_cast<int*>(e.err_flag.p),
+                                        static_cast<int>(st.features), static_cast<int*>(e.err_flag.p),
                                         e.stream),
                        "tile pass");
             break;

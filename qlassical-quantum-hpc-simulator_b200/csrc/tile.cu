@@ -696,7 +696,7 @@ __device__ __forceinline__ void op_cphase(float2 (&v)[NR], uint32_t cm, float2 p
 // 1-qubit rotations, diagonal, SWAP, U2 and tensor-core ops (kLevelTc);
 // everything, with the FP32 DENSE3-5 handlers (kLevelWide).  A pass runs the smallest that holds its ops: the
 // larger bodies cost instruction-fetch stalls.
-constexpr int kLevelNarrow = 0, kLevelSwaps = 1, kLevelTc = 2, kLevelWide = 3;
+constexpr int kLevelNarrow = kBodyNarrow, kLevelSwaps = kBodySwaps, kLevelTc = kBodyTc, kLevelWide = kBodyWide;
 
 // The op loop of one phase.  Each op is four 16-byte words; the first holds
 // the dispatch code, the register controls and the data offset.
@@ -1117,16 +1117,20 @@ cudaError_t configure_tile_kernel() {
 namespace {
 void launch_tile_kernel(unsigned grid, const TileWork& single, const TileWork* work, uint32_t n_work, uint64_t ntiles,
                         int features, int* err, cudaStream_t s) {
-    if (features & kPassWide)
+    switch (tile_body(features)) {
+    case kBodyWide:
         k_tile_pass<kLevelWide><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
-    else if ((features & (kPassTensorCores | kPassPairs)) && (features & kPassCtl))
-        k_tile_pass<kLevelWide><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
-    else if (features & (kPassTensorCores | kPassPairs))
+        break;
+    case kBodyTc:
         k_tile_pass<kLevelTc><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
-    else if (features & kPassSwaps)
+        break;
+    case kBodySwaps:
         k_tile_pass<kLevelSwaps><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
-    else
+        break;
+    default:
         k_tile_pass<kLevelNarrow><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
+        break;
+    }
 }
 }  // namespace
 

@@ -134,7 +134,7 @@ struct TilePass {
     uint8_t tile_pos[kTileQubits];    // tile-local position j -> memory qubit (ascending)
     uint8_t n_out;                    // number of non-tile qubits
     uint8_t n_low;                    // tile_pos[j] == j for j < n_low (>= kTileLow): runs of 2^n_low amps
-    uint8_t has_tc;                   // kernel features the pass needs (kPass* bits)
+    uint8_t features;                 // kernel features the pass needs (kPass* bits)
     uint8_t out_mem[40];              // non-tile memory qubits, ascending
     uint32_t phase_begin, phase_end;
 };
@@ -171,6 +171,32 @@ constexpr int kPassWide = 2;
 constexpr int kPassSwaps = 4;
 constexpr int kPassPairs = 8;
 constexpr int kPassCtl = 16;
+
+// Kernel bodies (instantiations of the tile kernel), smallest first: 1-qubit,
+// controlled and diagonal ops; those plus register SWAPs; uncontrolled
+// 1-qubit rotations, diagonal, SWAP, U2 and tensor-core ops; everything,
+// with the FP32 DENSE3-5 handlers.  A pass runs tile_body(features).
+constexpr int kBodyNarrow = 0, kBodySwaps = 1, kBodyTc = 2, kBodyWide = 3;
+constexpr int tile_body(int features) {
+    return (features & kPassWide) ? kBodyWide
+           : (features & (kPassTensorCores | kPassPairs)) ? ((features & kPassCtl) ? kBodyWide : kBodyTc)
+           : (features & kPassSwaps) ? kBodySwaps
+                                     : kBodyNarrow;
+}
+// Whether kernel body `body` has a handler for dispatch code `code` (the
+// planner checks every op of a pass against the body the pass will run).
+constexpr bool tile_body_handles(int body, uint32_t code) {
+    const bool common = (code >= OPC_U1 && code < OPC_SWAP) || code == OPC_DIAG || code == OPC_CPHASE;
+    const bool swap = code >= OPC_SWAP && code < OPC_U2;
+    const bool u2 = code >= OPC_U2 && code < OPC_DENSE3;
+    switch (body) {
+    case kBodyWide: return code >= OPC_U1 && code < OPC_COUNT;
+    case kBodyTc:
+        return (code >= OPC_U1 && code < OPC_X) || code == OPC_DIAG || swap || u2 || code == OPC_DENSE_TC;
+    case kBodySwaps: return common || swap;
+    default: return common;
+    }
+}
 
 // `err` (device int) receives a nonzero code if a bounded wait gave up.
 // `features`: the pass's kPass* bits (union over the entries of a work list).

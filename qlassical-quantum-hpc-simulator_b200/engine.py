@@ -291,3 +291,49 @@ class CUDAEngine:
         out = np.empty(int(shots), dtype=np.uint64)
         call("qlb_engine_sample", self._h, int(seed) & 0xFFFFFFFFFFFFFFFF, int(shots), _lib.ptr(out))
         return out
+
+
+class Check64:
+    """The FP64 checker (qlb_check64_*): a complex128 device state that runs
+    a program gate by gate in double precision, and compares itself with a
+    complex64 device state over the whole vector (max |delta| and
+    infidelity, reduced in FP64)."""
+
+    def __init__(self, num_qubits: int):
+        h = ctypes.c_void_p()
+        call("qlb_check64_create", ctypes.byref(h), int(num_qubits))
+        self._h = h
+        self.n = int(num_qubits)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().qlb_check64_destroy(h)
+            self._h = None
+
+    def close(self) -> None:
+        self.__del__()
+
+    def execute(self, program, pool: Optional[UnitaryPool] = None) -> None:
+        if isinstance(program, IRModule):
+            pool = program.unitaries()
+            program = program.program()
+        prog = np.ascontiguousarray(program, dtype=_lib.GATE_INSTR_DTYPE)
+        pool = pool if pool is not None else UnitaryPool()
+        pv, keep = pool.view()
+        call("qlb_check64_execute", self._h, _lib.ptr(prog), prog.size, ctypes.byref(pv))
+        del keep
+
+    def compare(self, engine: "CUDAEngine") -> dict:
+        """Compares with the engine's current device state (same size)."""
+        if engine.num_qubits() != self.n:
+            raise ValueError("the engine's qubit count differs from the checker's")
+        engine.synchronize()
+        r = _lib.Check64Result()
+        call("qlb_check64_compare", self._h, ctypes.c_void_p(engine.device_state()), ctypes.byref(r))
+        return r.as_dict()
+
+    def state(self) -> np.ndarray:
+        out = np.empty(1 << self.n, dtype=np.complex128)
+        call("qlb_check64_download", self._h, _lib.ptr(out), out.size)
+        return out

@@ -12,14 +12,16 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CPP_DIR = os.path.join(ROOT, "tests", "cpp")
 BIN = os.path.join(CPP_DIR, "_bin", "test_cuda_engine")
-REFERENCE_INCLUDE = "/root/reference/include"
+from oracle.oracle import REFERENCE_DIR  # noqa: E402  ($QLB_REFERENCE_DIR or `reference` beside the repo)
+
+REFERENCE_INCLUDE = os.path.join(REFERENCE_DIR, "include")
 
 
 @pytest.mark.skipif(not os.path.isdir(REFERENCE_INCLUDE), reason="reference headers absent")
 def test_dropin_compiles_against_reference_headers():
     """The headers compile in the reference's own include tree (C++20, -Wall)
     and the program links libqlassical_b200.so."""
-    r = subprocess.run(["make", "-s", "-C", CPP_DIR], capture_output=True, text=True)
+    r = subprocess.run(["make", "-s", "-C", CPP_DIR, f"REF={REFERENCE_DIR}"], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     assert os.path.isfile(BIN)
 

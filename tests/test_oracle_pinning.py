@@ -144,3 +144,47 @@ def test_qft_circuit_matches_analytic_dft():
         for x in (0, 1, (1 << n) - 3):
             s, _ = oracle.run_oracle(circuits.qft(n, basis_state=x))
             assert oracle.max_abs_diff(s, circuits.qft_expected(n, x)) < 1e-6
+
+
+@pytest.mark.parametrize("n,depth,seed", [(7, 3, 1), (12, 5, 1234), (30, 24, 1234)])
+def test_ref_workloads_match_package_circuits(n, depth, seed):
+    """bench.py's reference arm builds the benchmark circuit with numpy alone
+    (oracle/ref_workloads.py); its records and pool are byte-identical to the
+    package's circuit rewritten into the reference IR."""
+    from oracle import ref_workloads
+    rc = ref_workloads.random_rot_cz(n, depth, seed=seed)
+    m = circuits.to_reference_ir(circuits.random_rot_cz(n, depth, seed=seed))
+    assert rc.prog.tobytes() == m.program().tobytes()
+    pool = m.unitaries()
+    assert np.array_equal(rc.pool_data, pool.data)
+    assert rc.pool_meta.tobytes() == pool.metadata().tobytes()
+    assert rc.layer_starts == [i * (n + n // 2) for i in range(depth)]
+    one = rc.layers(2, 1)
+    assert one.gate_count() == n + n // 2
+    assert one.prog.tobytes() == m.program()[2 * (n + n // 2):3 * (n + n // 2)].tobytes()
+
+
+@pytest.mark.skipif(not oracle.reference_available(), reason="oracle/_ref not built")
+def test_ref_workloads_run_through_reference():
+    """The numpy-built reference IR runs through the reference engine (and
+    its transpiler) and agrees with the oracle on the package's circuit."""
+    from oracle import ref_workloads
+    rc = ref_workloads.random_rot_cz(9, 4, seed=3)
+    a, _ = oracle.run_reference(rc, seed=1)
+    b, _ = oracle.run_oracle(circuits.random_rot_cz(9, 4, seed=3))
+    assert oracle.max_abs_diff(a, b) < 1e-12
+    prog, data, meta = oracle.transpile_reference(rc, fusion=True, hw=False)
+    fused = ref_workloads.RefCircuit(9, prog, data, meta)
+    c, _ = oracle.run_reference(fused, seed=1)
+    assert oracle.max_abs_diff(a, c) < 1e-10
+    assert oracle.time_reference(fused, reps=1) > 0.0
+
+
+@pytest.mark.parametrize("n", [3, 8, 33])
+def test_ref_workloads_qft_matches_package(n):
+    from oracle import ref_workloads
+    rc = ref_workloads.qft(n)
+    m = circuits.to_reference_ir(circuits.qft(n))
+    assert rc.prog.tobytes() == m.program().tobytes()
+    assert np.array_equal(rc.pool_data, m.unitaries().data)
+    assert rc.pool_meta.tobytes() == m.unitaries().metadata().tobytes()

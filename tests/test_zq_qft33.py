@@ -1,7 +1,8 @@
 """The 33-qubit QFT (68.7 GB complex64 state) against the analytic result:
 QFT|x> has amplitudes exp(2 pi i ((x*k) mod 2^33) / 2^33) / 2^16.5, whose
 phase index is exact in integer arithmetic.  Checked on seeded random
-amplitudes gathered on the device, plus the FP64 norm of the whole state.
+amplitudes gathered on the device (per-amplitude relative error and the
+sampled infidelity <= 1e-6), plus the FP64 norm of the whole state.
 Runs only on a GPU with room for the state."""
 import math
 
@@ -41,6 +42,11 @@ def test_qft33_matches_analytic(x):
     want = np.exp(2j * np.pi * ph) / math.sqrt(float(1 << N))
     rel = np.abs(got - want) * math.sqrt(float(1 << N))
     assert rel.max() < 2e-3, rel.max()
+    # sampled infidelity 1 - |<want|got>|^2 / (<want|want><got|got>) over the
+    # gathered amplitudes, against the stated bound
+    ov = np.vdot(want, got)
+    infid = 1.0 - abs(ov) ** 2 / (np.vdot(want, want).real * np.vdot(got, got).real)
+    assert infid <= 1e-6, infid
     st = eng.last_stats()
     assert st["tile_passes"] <= 8
     del eng

@@ -28,6 +28,29 @@ def _noalloc(engine, n):
     return out
 
 
+def _free_bytes():
+    free = ctypes.c_uint64()
+    total = ctypes.c_uint64()
+    sm = ctypes.c_int()
+    _lib.call("qlb_device_info", ctypes.byref(sm), ctypes.byref(free), ctypes.byref(total))
+    return free.value
+
+
+def test_noalloc_takes_no_memory_after_its_warm_up_call():
+    """The first call commits the fixed scratch; later calls change the
+    device's free memory by nothing."""
+    n = 18
+    e = q.CUDAEngine(n, seed=1)
+    e.execute(circuits.random_rot_cz(n, 3, seed=2))
+    e.expect_z()             # the allocating path's scratch exists before we measure
+    _noalloc(e, n)           # warm-up: commits the scratch on this device
+    e.synchronize()
+    before = _free_bytes()
+    for _ in range(3):
+        _noalloc(e, n)
+    assert _free_bytes() == before
+
+
 @pytest.mark.parametrize("n", [9, 22, 16])
 def test_noalloc_matches_allocating_reduction_twice(n):
     m = circuits.random_rot_cz(n, 4, seed=n)
