@@ -58,5 +58,5 @@ def test_check64_rejects_measure():
     qc.h(0)
     qc.measure(0)
     c = q.Check64(4)
-    with pytest.raises(q.QlbError):
+    with pytest.raises(ValueError):          # QLB_ERR_INVALID_ARG
         c.execute(qc.release())
