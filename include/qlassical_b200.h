@@ -167,8 +167,13 @@ int qlb_engine_get_mode(qlb_engine_t e, int* mode);
  * data movement.  QLB_OPT_TC_MIN_COST (TILED_TC only): a run of
  * register-local ops goes to the tensor cores when its estimated CUDA-core
  * cost, in hundredths of an instruction per amplitude, reaches the value
- * (default 1000); cheaper runs stay on the CUDA cores. */
-enum qlb_option { QLB_OPT_PHYSICAL_GLOBAL_SWAP = 1, QLB_OPT_TC_MIN_COST = 2 };
+ * (default 1000); cheaper runs stay on the CUDA cores.  QLB_OPT_TC_CHAIN
+ * (TILED_TC only, default 1): a register phase whose ops are all uniform
+ * over the tile becomes one tensor-core op whatever its cost, and a pass
+ * made only of such phases runs on the tensor-core chain kernel (two tiles
+ * in flight per SM, loads by a dedicated warp); 0 keeps every pass on the
+ * general tile kernel. */
+enum qlb_option { QLB_OPT_PHYSICAL_GLOBAL_SWAP = 1, QLB_OPT_TC_MIN_COST = 2, QLB_OPT_TC_CHAIN = 3 };
 int qlb_engine_set_option(qlb_engine_t e, int key, int64_t value);
 int qlb_engine_synchronize(qlb_engine_t e);
 /* The device state pointer (float2 *) and the stream the engine launches on. */
@@ -184,6 +189,7 @@ typedef struct qlb_exec_stats {
     uint64_t dense_ops;         /* dense unitaries applied */
     uint64_t tc_ops;            /* dense unitaries applied on the tensor cores */
     double   sweep_bytes;       /* algorithmic bytes: 16 B/amp per full sweep */
+    uint64_t chain_passes;      /* tiled passes run by the tensor-core chain kernel */
 } qlb_exec_stats;
 int qlb_engine_last_stats(qlb_engine_t e, qlb_exec_stats* out);
 

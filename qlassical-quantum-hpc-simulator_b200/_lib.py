@@ -82,6 +82,7 @@ class ExecStats(ctypes.Structure):
         ("dense_ops", ctypes.c_uint64),
         ("tc_ops", ctypes.c_uint64),
         ("sweep_bytes", ctypes.c_double),
+        ("chain_passes", ctypes.c_uint64),
     ]
 
     def as_dict(self):

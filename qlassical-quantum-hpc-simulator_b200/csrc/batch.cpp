@@ -86,7 +86,7 @@ std::unique_ptr<BatchProgram> build_program(qlb_batch& b, int mode, const qlb_ga
         auto worker = [&] {
             for (uint32_t c; (c = next.fetch_add(1)) < C;) {
                 try {
-                    const PlanConfig cfg{b.states[c].eff_qubits, mode, 0, 10.0};
+                    const PlanConfig cfg{b.states[c].eff_qubits, mode, 0, 10.0, 0};   // work lists: no chain kernel
                     plans[c] = plan_host(cfg, programs[c], counts[c], &pools[c]);
                 } catch (const Error& e) {
                     codes[c] = e.code;

@@ -1,0 +1,425 @@
+// chain.cu -- the tensor-core chain kernel: one launch per chain pass.
+//
+// A chain pass is a tile pass whose register phases each hold one op, a
+// 32 x 32 complex unitary on the phase's five register qubits applied by
+// tcgen05 split-bf16 MMAs (A = the tile, 256 rows; B = the unitary's real
+// embedding, hi/lo; FP32 accumulate in tensor memory; the operand layouts
+// are the general tile kernel's, tile.cu).  Between two ops the tile never
+// visits the register file longer than one conversion: tensor memory ->
+// registers (D1 + D2) -> bf16 hi/lo -> the next op's A operand in shared
+// memory, scattered by the planner's per-bit XOR offsets.
+//
+// Where the general kernel runs one tile at a time and waits for every
+// MMA, this one keeps two tiles in flight per SM ("slots", each with 256
+// tensor-memory columns and its own B staging): while slot 0's MMAs run,
+// the 256 compute threads convert slot 1's tile, and the other way round.
+// Slot 1 starts half a tile behind slot 0, so its buffer's next load has
+// time to land.  A ninth warp does nothing but load tiles (cp.async 16 B
+// pieces, or TMA bulk copies for runs >= 4 KB) into three 64 KB buffers,
+// two tiles ahead; a buffer is reloaded when the last MMA that read it as
+// an A operand completes.  Tiles are stored from registers after the last
+// op.  HBM traffic: 16 B per amplitude per pass.
+//
+// Every wait is bounded (2 s / 2^26 polls); on expiry the CTA raises *err,
+// waits (bounded) for its own MMAs and copies, frees its tensor memory and
+// returns.
+#include "common.cuh"
+#include "tc_ptx.cuh"
+#include "tile.h"
+
+namespace qlb {
+
+namespace {
+
+using namespace ptx;
+
+constexpr int kCompute = 256;                     // thread t converts A / D row t
+constexpr int kThreads = kCompute + 32;           // + the load warp
+constexpr uint32_t kTile = 1u << kTileQubits;
+constexpr uint32_t kBufBytes = kTile * 8u;        // 64 KB: the tile (fp32) or its A operand (bf16 hi | lo)
+constexpr uint32_t kBufs = 3;
+constexpr uint32_t kBulkMin = 9;                  // runs of >= 2^9 amplitudes move by bulk copies
+constexpr size_t kOffB = size_t{kBufs} * kBufBytes;
+constexpr size_t kOffPass = kOffB + 2 * kTcBBytes;
+constexpr size_t kOffPhases = kOffPass + sizeof(TilePass);
+constexpr size_t kOffBoff = kOffPhases + kMaxSmemPhases * sizeof(TilePhase);
+constexpr size_t kOffBar = (kOffBoff + kMaxSmemPhases * 4 + 7) & ~size_t{7};
+constexpr size_t kSmemChain = kOffBar + 9 * 8 + 8;
+static_assert(sizeof(TilePass) % 8 == 0 && sizeof(TilePhase) % 4 == 0, "descriptor staging");
+static_assert(kSmemChain <= 227 * 1024, "shared memory per CTA");
+constexpr uint32_t kBPerThread = kTcBBytes / (16u * kCompute);   // 4 x 16 B of B per thread
+constexpr uint32_t kTmemCols = 512;               // two slots x (2 M-blocks x (D1 | D2))
+
+__device__ __forceinline__ uint64_t tile_base(const TilePass& P, uint64_t tile) {
+    uint64_t base = 0;
+    for (uint32_t j = 0; j < P.n_out; ++j, tile >>= 1)
+        if (tile & 1u) base |= uint64_t{1} << P.out_mem[j];
+    return base;
+}
+
+// Barrier 1 over the 256 compute threads (the load warp never joins it).
+__device__ __forceinline__ void compute_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+__device__ __forceinline__ bool compute_any(bool x) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, 1, 256, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"(x ? 1u : 0u)
+        : "memory");
+    return r != 0;
+}
+
+// Issues the 16 MMAs of one op on A at `a` (hi; lo 32 KB above), B at `b`,
+// D at tensor-memory column `d`: per M-block of 128 rows, A_hi x [B_hi |
+// B_lo] (N = 128) into D1 | D2, then A_lo x B_hi (N = 64) added into D1.
+__device__ __forceinline__ void issue_mmas(uint32_t a, uint32_t b, uint32_t d, uint64_t* bar) {
+    tc_fence_after();
+#pragma unroll
+    for (uint32_t mb = 0; mb < 2; ++mb) {
+        const uint32_t dm = d + mb * 128u;
+#pragma unroll
+        for (uint32_t s = 0; s < 4; ++s)
+            tc_mma(dm, umma_desc_a(a + mb * 16384u + s * 32u), umma_desc_b(b + s * 256u), kTcIdesc128, s > 0 ? 1u : 0u);
+#pragma unroll
+        for (uint32_t s = 0; s < 4; ++s)
+            tc_mma(dm, umma_desc_a(a + 32768u + mb * 16384u + s * 32u), umma_desc_b(b + s * 256u), kTcIdesc64, 1u);
+    }
+    tc_commit(bar);
+}
+
+// Reads 16 amplitudes (register indices 16 h .. 16 h + 15) of this thread's
+// D row: D1 + D2, columns 32 h .. 32 h + 31 of each.
+__device__ __forceinline__ void read_half(uint32_t row, uint32_t h, float2 (&a)[16]) {
+    uint32_t r1[32], r2[32];
+    tc_ld_32(row + h * 32u, r1);
+    tc_ld_32(row + 64u + h * 32u, r2);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int c = 0; c < 16; ++c)
+        a[c] = make_float2(__uint_as_float(r1[2 * c]) + __uint_as_float(r2[2 * c]),
+                           __uint_as_float(r1[2 * c + 1]) + __uint_as_float(r2[2 * c + 1]));
+}
+
+// Scatters amplitudes with register indices base_r .. base_r + 15 into the
+// A operand at `a` (hi; lo 32 KB above): byte offset = thread part ^ XOR of
+// d[i] over the index's set bits.
+__device__ __forceinline__ void scatter16(const float2 (&v)[16], uint32_t base_r, uint32_t thr_off,
+                                          const uint32_t (&d)[kRegQubits], unsigned char* a) {
+#pragma unroll
+    for (uint32_t c = 0; c < 16; ++c) {
+        const uint32_t r = base_r + c;
+        uint32_t off = thr_off;
+#pragma unroll
+        for (int i = 0; i < kRegQubits; ++i)
+            if ((r >> i) & 1u) off ^= d[i];
+        uint32_t hi, lo;
+        tc_split(v[c], hi, lo);
+        *reinterpret_cast<uint32_t*>(a + off) = hi;
+        *reinterpret_cast<uint32_t*>(a + 32768u + off) = lo;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char* bufs = smem;
+    unsigned char* bstage = smem + kOffB;
+    TilePass* sp = reinterpret_cast<TilePass*>(smem + kOffPass);
+    TilePhase* sph = reinterpret_cast<TilePhase*>(smem + kOffPhases);
+    uint32_t* sboff = reinterpret_cast<uint32_t*>(smem + kOffBoff);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + kOffBar);    // [3] tile loaded
+    uint64_t* empty = full + 3;                                      // [3] buffer free again
+    uint64_t* mmab = full + 6;                                       // [2] a slot's MMAs done
+    uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(full + 8);
+    const uint32_t tid = threadIdx.x;
+
+    // ---- set-up: the pass descriptor, its phases, the ops' B offsets ----
+    {
+        const TilePass& GP = w.passes[w.pass];
+        for (uint32_t i = tid; i < sizeof(TilePass) / 4; i += kThreads)
+            reinterpret_cast<uint32_t*>(sp)[i] = reinterpret_cast<const uint32_t*>(&GP)[i];
+        const uint32_t pb = GP.phase_begin, np = GP.phase_end - pb;
+        for (uint32_t i = tid; i < np * (sizeof(TilePhase) / 4); i += kThreads)
+            reinterpret_cast<uint32_t*>(sph)[i] = reinterpret_cast<const uint32_t*>(w.phases + pb)[i];
+        if (tid < np) {
+            const TilePhase& ph = w.phases[pb + tid];
+            sboff[tid] = ph.op_end > ph.op_begin ? w.ops[ph.op_begin].data : 0u;
+        }
+    }
+    if (tid == 0) {
+        for (int b = 0; b < 3; ++b) {
+            mbar_init(&full[b], 32);     // one (deferred) arrival per load-warp lane
+            mbar_init(&empty[b], 1);
+        }
+        mbar_init(&mmab[0], 1);
+        mbar_init(&mmab[1], 1);
+        fence_mbar_init();
+    }
+    if (tid < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_holder)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_holder;
+    const TilePass& P = *sp;
+    const uint32_t nph = P.phase_end - P.phase_begin;
+    const uint32_t first = sph[0].op_end > sph[0].op_begin ? 0u : 1u;
+    const uint32_t last = sph[nph - 1].op_end > sph[nph - 1].op_begin ? nph - 1 : nph - 2;
+    const uint32_t m = last - first + 1;           // tensor-core ops per tile
+
+    if (tid >= kCompute) {
+        // ---- the load warp ---------------------------------------------------
+        const uint32_t lane = tid - kCompute;
+        const uint32_t nl = P.n_low;
+        bool ok = true;
+        // cp.async pieces: lane l, piece c covers tile-local amplitudes 2 i,
+        // 2 i + 1 with i = l + 32 c (bits 1..5 from the lane, 6..12 from c).
+        uint64_t gl = 0, hb[7];
+#pragma unroll
+        for (int i = 0; i < 5; ++i)
+            if ((lane >> i) & 1u) gl |= uint64_t{1} << P.tile_pos[1 + i];
+#pragma unroll
+        for (int i = 0; i < 7; ++i) hb[i] = uint64_t{1} << P.tile_pos[6 + i];
+        for (uint32_t k = 0;; ++k) {
+            const uint64_t tile = blockIdx.x + static_cast<uint64_t>(k) * gridDim.x;
+            if (tile >= ntiles) break;
+            const uint32_t b = k % kBufs;
+            if (k >= kBufs && !mbar_wait_bounded(&empty[b], ((k / kBufs) - 1u) & 1u)) {
+                ok = false;
+                break;
+            }
+            unsigned char* dst = bufs + b * kBufBytes;
+            const uint64_t base = tile_base(P, tile);
+            const float2* __restrict__ state = w.state;
+            if (nl >= kBulkMin) {
+                const uint32_t chunks = 1u << (kTileQubits - nl);
+                const uint32_t bytes = (1u << nl) * 8u;
+                if (lane == 0) mbar_arrive_expect_tx(&full[b], kBufBytes);
+                for (uint32_t c = lane; c < chunks; c += 32) {
+                    uint64_t g = base;
+                    for (uint32_t j = nl; j < static_cast<uint32_t>(kTileQubits); ++j)
+                        if ((c >> (j - nl)) & 1u) g |= uint64_t{1} << P.tile_pos[j];
+                    bulk_g2s(dst + (static_cast<size_t>(c) << nl) * 8u, state + g, bytes, &full[b]);
+                }
+                if (lane != 0) mbar_arrive(&full[b]);
+            } else {
+                uint64_t g = base | gl;
+                uint32_t d = smem_u32(dst) + 16u * lane;
+                // pieces in Gray-code order of c: one address bit changes per
+                // step (bits 0..2 inside a group of 8, bits 3..6 between groups)
+#pragma unroll 1
+                for (uint32_t hi = 0; hi < 16; ++hi) {
+                    if (hi) {
+                        const uint32_t bit = static_cast<uint32_t>(__ffs(static_cast<int>(hi))) - 1u;   // 0..3
+                        g ^= bit == 0 ? hb[3] : bit == 1 ? hb[4] : bit == 2 ? hb[5] : hb[6];
+                        d ^= 4096u << bit;
+                    }
+#pragma unroll
+                    for (uint32_t lo = 0; lo < 8; ++lo) {
+                        if (lo) {   // lowest set bit of lo: the bit that flips
+                            const uint32_t bit = (lo & 1u) ? 0u : (lo & 2u) ? 1u : 2u;
+                            g ^= hb[bit];
+                            d ^= 512u << bit;
+                        }
+                        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(state + g) : "memory");
+                    }
+                    // back to lo = 0 of this group's Gray sequence: 0,1,3,2,6,7,5,4 ends at 4
+                    g ^= hb[2];
+                    d ^= 2048u;
+                }
+                asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(&full[b]))
+                             : "memory");
+            }
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        if (!ok && lane == 0) atomicExch(err, 4);
+    } else {
+        // ---- the compute warps: two slots, one step each per round -----------
+        const uint32_t t = tid;
+        const uint32_t wq = t >> 5;
+        const uint32_t drow = ((wq & 3u) * 32u) << 16 | ((wq >> 2) * 128u);   // lane quarter, M-block
+        uint32_t kk[2] = {0u, 1u};
+        int jj[2] = {0, -static_cast<int>((m + 1u) / 2u)};
+        uint32_t uses[2] = {0u, 0u};
+        bool pending[2] = {false, false};
+        bool failed = false;
+        const float2* __restrict__ mats = w.mats;
+        float2* __restrict__ state = w.state;
+        for (;;) {
+            bool active = false;
+#pragma unroll 1
+            for (uint32_t s = 0; s < 2 && !failed; ++s) {
+                const uint64_t tile = blockIdx.x + static_cast<uint64_t>(kk[s]) * gridDim.x;
+                if (tile >= ntiles) continue;
+                active = true;
+                if (jj[s] < 0) {
+                    ++jj[s];
+                    continue;
+                }
+                const uint32_t j = static_cast<uint32_t>(jj[s]);
+                const uint32_t b = kk[s] % kBufs;
+                unsigned char* buf = bufs + b * kBufBytes;
+                unsigned char* bs = bstage + s * kTcBBytes;
+                const uint32_t dcol = tmem + 256u * s;
+                // B of the op this step issues (L2-resident; its load latency
+                // hides behind the wait and the conversion)
+                uint4 bq[kBPerThread];
+                if (j < m) {
+                    const uint4* bsrc = reinterpret_cast<const uint4*>(mats + sboff[first + j]);
+#pragma unroll
+                    for (uint32_t i = 0; i < kBPerThread; ++i) bq[i] = __ldg(bsrc + i * kCompute + t);
+                }
+                if (j == 0) {
+                    // the loaded tile -> A of the first op
+                    const bool ok = mbar_wait_bounded(&full[b], (kk[s] / kBufs) & 1u);
+                    if (compute_any(!ok)) {
+                        failed = true;
+                        if (t == 0) atomicExch(err, 1);
+                        break;
+                    }
+                    const TilePhase& R = sph[0];
+                    uint32_t tp = 0, e[kRegQubits];
+#pragma unroll
+                    for (int i = 0; i < kThreadQubits; ++i)
+                        if ((t >> i) & 1u) tp |= 1u << R.thr_pos[i];
+#pragma unroll
+                    for (int i = 0; i < kRegQubits; ++i) e[i] = 1u << R.reg_pos[i];
+                    const float2* src = reinterpret_cast<const float2*>(buf);
+                    float2 v[32];
+#pragma unroll
+                    for (int r = 0; r < 32; ++r) {
+                        uint32_t l = tp;
+#pragma unroll
+                        for (int i = 0; i < kRegQubits; ++i)
+                            if ((r >> i) & 1) l |= e[i];
+                        v[r] = src[l];
+                    }
+                    compute_sync();      // every thread has read the tile: the buffer becomes A
+                    if (first == 0) {
+                        tc_write_a(v, buf, buf + 32768u);   // own row, identity K order
+                    } else {
+                        const TilePhase& F = sph[first];
+                        uint32_t thr = 0, d[kRegQubits];
+#pragma unroll
+                        for (int i = 0; i < kThreadQubits; ++i)
+                            if ((t >> i) & 1u) thr ^= F.a_thr[i];
+#pragma unroll
+                        for (int i = 0; i < kRegQubits; ++i) d[i] = F.a_reg[i];
+                        float2 h0[16], h1[16];
+#pragma unroll
+                        for (int c = 0; c < 16; ++c) {
+                            h0[c] = v[c];
+                            h1[c] = v[16 + c];
+                        }
+                        scatter16(h0, 0u, thr, d, buf);
+                        scatter16(h1, 16u, thr, d, buf);
+                    }
+                } else {
+                    const bool ok = mbar_wait_bounded(&mmab[s], uses[s] & 1u);
+                    ++uses[s];
+                    pending[s] = false;
+                    if (compute_any(!ok)) {
+                        failed = true;
+                        if (t == 0) atomicExch(err, 2);
+                        break;
+                    }
+                    tc_fence_after();
+                    if (j == m) {
+                        // the last op's result -> HBM; the buffer is free once its MMAs are done
+                        if (t == 0) mbar_arrive(&empty[b]);
+                        const TilePhase& L = sph[last];
+                        uint64_t gt = tile_base(P, tile), ge[kRegQubits];
+#pragma unroll
+                        for (int i = 0; i < kThreadQubits; ++i)
+                            if ((t >> i) & 1u) gt |= uint64_t{1} << P.tile_pos[L.thr_pos[i]];
+#pragma unroll
+                        for (int i = 0; i < kRegQubits; ++i) ge[i] = uint64_t{1} << P.tile_pos[L.reg_pos[i]];
+#pragma unroll
+                        for (uint32_t h = 0; h < 2; ++h) {
+                            float2 a[16];
+                            read_half(dcol + drow, h, a);
+#pragma unroll
+                            for (uint32_t c = 0; c < 16; ++c) {
+                                const uint32_t r = 16u * h + c;
+                                uint64_t g = gt;
+#pragma unroll
+                                for (int i = 0; i < kRegQubits; ++i)
+                                    if ((r >> i) & 1u) g |= ge[i];
+                                state[g] = a[c];
+                            }
+                        }
+                        tc_fence_before();
+                        kk[s] += 2;
+                        jj[s] = 0;
+                        continue;
+                    }
+                    // D of op j - 1 -> A of op j
+                    const TilePhase& F = sph[first + j];
+                    uint32_t thr = 0, d[kRegQubits];
+#pragma unroll
+                    for (int i = 0; i < kThreadQubits; ++i)
+                        if ((t >> i) & 1u) thr ^= F.a_thr[i];
+#pragma unroll
+                    for (int i = 0; i < kRegQubits; ++i) d[i] = F.a_reg[i];
+#pragma unroll
+                    for (uint32_t h = 0; h < 2; ++h) {
+                        float2 a[16];
+                        read_half(dcol + drow, h, a);
+                        scatter16(a, 16u * h, thr, d, buf);
+                    }
+                }
+                // B into this slot's staging (its previous MMAs are done), then
+                // A and B go to the tensor core
+                uint4* bdst = reinterpret_cast<uint4*>(bs);
+#pragma unroll
+                for (uint32_t i = 0; i < kBPerThread; ++i) bdst[i * kCompute + t] = bq[i];
+                fence_proxy_async();
+                tc_fence_before();
+                compute_sync();
+                if (t == 0) issue_mmas(smem_u32(buf), smem_u32(bs), dcol, &mmab[s]);
+                pending[s] = true;
+                jj[s] = static_cast<int>(j) + 1;
+            }
+            if (!active || failed) break;
+        }
+        // MMAs still in flight (only after a failure) complete before the
+        // tensor memory is released
+        for (uint32_t s = 0; s < 2; ++s)
+            if (pending[s]) mbar_wait_bounded(&mmab[s], uses[s] & 1u);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (tid < 32) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_chain_pass(float2* state, uint32_t n, const TilePass* d_passes, const TilePhase* d_phases,
+                              const TileOp* d_ops, const float2* d_mats, uint32_t pass_index, int* err,
+                              cudaStream_t s) {
+    static bool configured = false;
+    if (!configured) {
+        const cudaError_t e = cudaFuncSetAttribute(k_tc_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   static_cast<int>(kSmemChain));
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    const uint64_t tiles = uint64_t{1} << (n - kTileQubits);
+    uint64_t grid = static_cast<uint64_t>(sm_count());
+    if (grid > tiles) grid = tiles;
+    const TileWork w{state, 0, d_passes, d_phases, d_ops, d_mats, pass_index, 0};
+    k_tc_chain<<<static_cast<unsigned>(grid), kThreads, kSmemChain, s>>>(w, tiles, err);
+    return cudaGetLastError();
+}
+
+}  // namespace qlb

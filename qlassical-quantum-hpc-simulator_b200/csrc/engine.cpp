@@ -683,6 +683,8 @@ int qlb_engine_set_option(qlb_engine_t e, int key, int64_t value) {
         } else if (key == QLB_OPT_TC_MIN_COST) {
             if (value < 0) fail(QLB_ERR_INVALID_ARG, "QLB_OPT_TC_MIN_COST must be >= 0");
             e->tc_min_cost = static_cast<double>(value) / 100.0;
+        } else if (key == QLB_OPT_TC_CHAIN) {
+            e->tc_chain = value != 0;
         } else {
             fail(QLB_ERR_INVALID_ARG, "unknown engine option");
         }

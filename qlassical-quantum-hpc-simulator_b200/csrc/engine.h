@@ -68,6 +68,7 @@ struct qlb_engine {
     int mode = QLB_MODE_TILED;
     int physical_global_swap = 0;   // execute GLOBAL_SWAP as a data permutation
     double tc_min_cost = 10.0;      // TILED_TC: smallest fused-run cost sent to the tensor cores
+    int tc_chain = 1;               // TILED_TC: chain kernel for passes of tensor-core ops only
     qlb::DeviceBuffer red_partial, red_out, staging, err_flag, exec_plan;   // exec_plan: execute()'s plan image   // err_flag: device int set by bounded waits
     qlb::PinnedBuffer host_pinned, host_prog;
     qlb_exec_stats stats{};

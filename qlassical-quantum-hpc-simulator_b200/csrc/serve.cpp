@@ -407,7 +407,7 @@ int qlb_server_submit(qlb_server_t s, const qlb_gate_instr* program, uint64_t co
         r->neff = std::max(num_qubits, kBatchMinQubits);
         r->shots = shots;
         r->seed = seed;
-        r->plan = plan_host(PlanConfig{r->neff, s->mode, 0, 10.0}, program, count, pool ? pool : &empty);
+        r->plan = plan_host(PlanConfig{r->neff, s->mode, 0, 10.0, 0}, program, count, pool ? pool : &empty);
         for (const PlanStep& st : r->plan.steps)
             if (st.kind != STEP_PASS)
                 fail(QLB_ERR_INVALID_ARG, "served circuits may hold only gates (no MEASURE, no 6-qubit blocks)");

@@ -629,6 +629,7 @@ private:
                 choose_kperm(*prev, ph, entry_kperm_);
                 entry_op_ = ph.op_begin;
             }
+            phase_ops_begin_ = ph.op_begin;
             encode_ops(pb, P, local_of, final_pass && pi + 1 == phases.size());
             entry_op_ = ~0u;
             ph.op_end = static_cast<uint32_t>(prog.ops.size());
@@ -642,6 +643,10 @@ private:
         P.phase_end = static_cast<uint32_t>(prog.phases.size());
         P.n_low = 0;
         while (P.n_low < kTileQubits && P.tile_pos[P.n_low] == P.n_low) ++P.n_low;
+        if (chain_form(P)) {
+            pass_features_ |= kPassChain;
+            stats.chain_passes += 1;
+        }
         P.features = static_cast<uint8_t>(pass_features_);
         // Every op must have a handler in the body the pass will run (a
         // missing one would be skipped by the kernel's dispatch).
@@ -661,6 +666,43 @@ private:
         stats.tile_passes += 1;
         stats.sweeps += 1;
         stats.launches += 1;
+    }
+
+    // A pass the tensor-core chain kernel can run: every register phase holds
+    // exactly one op, a tensor-core op -- phase 0 (applied in its own layout,
+    // identity K order) or an entry phase -- except an empty load phase
+    // first and an empty store phase last.  Phase 0's entry offsets are
+    // filled for its own layout so the chain kernel treats every op alike.
+    bool chain_form(TilePass& P) {
+        if (e_.mode != QLB_MODE_TILED_TC || !e_.tc_chain) return false;
+        const uint32_t pb = P.phase_begin, pe = static_cast<uint32_t>(prog.phases.size());
+        const uint32_t nph = pe - pb;
+        if (nph == 0 || nph > kMaxSmemPhases) return false;
+        auto nops = [&](uint32_t i) { return prog.phases[i].op_end - prog.phases[i].op_begin; };
+        auto tc_only = [&](uint32_t i) { return nops(i) == 1 && prog.ops[prog.phases[i].op_begin].kind == TOP_DENSE_TC; };
+        uint32_t first = pb;
+        if (nops(pb) == 0) {
+            first = pb + 1;
+            if (first >= pe || !(prog.phases[first].flags & kPhaseTcEntry)) return false;
+        }
+        if (!tc_only(first)) return false;
+        uint32_t last = first;
+        for (uint32_t i = first + 1; i < pe; ++i) {
+            if (nops(i) == 0 && i + 1 == pe) break;                 // store phase
+            if (!tc_only(i) || !(prog.phases[i].flags & kPhaseTcEntry)) return false;
+            last = i;
+        }
+        (void)last;
+        if (first == pb) {
+            static const int ident[kRegQubits] = {0, 1, 2, 3, 4};
+            TilePhase& ph = prog.phases[pb];
+            const uint32_t kp = prog.ops[ph.op_begin].flags;       // 3 bits per register bit
+            for (int j = 0; j < kRegQubits; ++j)
+                if (((kp >> (3 * j)) & 7u) != static_cast<uint32_t>(j)) return false;   // identity K order
+            for (int j = 0; j < kThreadQubits; ++j) ph.a_thr[j] = a_offset(ph, ident, ph.thr_pos[j]);
+            for (int j = 0; j < kRegQubits; ++j) ph.a_reg[j] = a_offset(ph, ident, ph.reg_pos[j]);
+        }
+        return true;
     }
 
     int reg_bit(const PhaseBuild& pb, const int* local_of, uint32_t memq) const {
@@ -685,6 +727,7 @@ private:
     // RZ and diagonal UNITARYs); applied once at the end of its last phase.
     double pass_global_ = 0.0;
     int pass_features_ = 0;   // kPass* bits of the pass being built
+    uint32_t phase_ops_begin_ = 0;   // first op of the phase being encoded
     // A tensor-core op emitted as op entry_op_ opens a kPhaseTcEntry
     // candidate phase and takes the K permutation entry_kperm_.
     uint32_t entry_op_ = ~0u;
@@ -957,9 +1000,12 @@ private:
         double cost = 0.0;
     };
 
-    void flush(Acc& acc) {
+    // `whole_phase`: the run is everything the phase holds; with the chain
+    // kernel on it goes to the tensor cores whatever its cost (the phase is
+    // then a single tensor-core op, which a chain pass is made of).
+    void flush(Acc& acc, bool whole_phase = false) {
         if (acc.ops.empty()) return;
-        if (acc.cost < e_.tc_min_cost) {     // cheaper as individual CUDA-core ops
+        if (acc.cost < e_.tc_min_cost && !(whole_phase && e_.tc_chain)) {   // cheaper as CUDA-core ops
             for (const HostOp& h : acc.ops) emit_cuda_op(h);
         } else {
             std::vector<cd> U(32 * 32, cd(0.0, 0.0));
@@ -1342,7 +1388,7 @@ private:
         }
         flush_rotations();
         if (last_phase) flush_pending(pb, local_of, tc ? &acc : nullptr, true);
-        if (tc) flush(acc);
+        if (tc) flush(acc, prog.ops.size() == phase_ops_begin_);
     }
 };
 
@@ -1363,7 +1409,7 @@ HostPlan plan_host(const PlanConfig& cfg, const qlb_gate_instr* prog, uint64_t c
 
 qlb_plan* compile_plan(qlb_engine& e, const qlb_gate_instr* prog, uint64_t count, const qlb_pool_view* pool,
                        DeviceBuffer* image) {
-    Planner pl(PlanConfig{e.sv.n, e.mode, e.physical_global_swap, e.tc_min_cost}, pool);
+    Planner pl(PlanConfig{e.sv.n, e.mode, e.physical_global_swap, e.tc_min_cost, e.tc_chain}, pool);
     pl.plan(prog, count);
     TileProgram& tp = pl.prog;
     auto* p = new qlb_plan();
@@ -1527,6 +1573,8 @@ std::string describe_plan_json(const PlanConfig& cfg, const qlb_gate_instr* prog
     u(pl.stats.tile_passes);
     out += ",\"tc_ops\":";
     u(pl.stats.tc_ops);
+    out += ",\"chain_passes\":";
+    u(pl.stats.chain_passes);
     out += ",\"dense_ops\":";
     u(pl.stats.dense_ops);
     out += ",\"ops\":";

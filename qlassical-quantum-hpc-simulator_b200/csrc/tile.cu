@@ -18,16 +18,19 @@
 #include <cuda_bf16.h>
 
 #include "common.cuh"
+#include "tc_ptx.cuh"
 #include "tile.h"
 
 namespace qlb {
 
 namespace {
 
+using namespace ptx;
+constexpr uint32_t kTcCols = 256;               // per M-block: D1 (64 columns) | D2 (64 columns)
+
 constexpr int NT = kTileThreads;            // 256
 constexpr int NR = 1 << kRegQubits;         // 32
 constexpr int TILE = 1 << kTileQubits;      // 8192
-constexpr uint32_t kWaitLimit = 1u << 26;
 // Tiles whose contiguous runs are at least 2^9 amplitudes (4 KB) move by TMA
 // bulk copies (at most 16 per tile) in both directions; shorter runs load by
 // cp.async and store from registers.
@@ -40,64 +43,6 @@ constexpr size_t kSmemTcB = 16384;           // B operand staging of a tensor-co
 constexpr size_t kSmemTotal = kSmemBuffers + kSmemOps + kSmemPhases + sizeof(TilePass) + kSmemMisc + kSmemTcB;
 static_assert((kSmemBuffers + kSmemOps + kSmemPhases + sizeof(TilePass)) % 16 == 0, "mbarriers and B staging alignment");
 static_assert(kSmemTotal <= 227 * 1024, "shared memory per CTA");
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ uint64_t global_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-// Gives up after kWaitLimit polls or `limit_ns` (2 s), whichever comes first.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
-                                                  uint64_t limit_ns = 2000000000ull) {
-    const uint64_t t0 = global_ns();
-    for (uint32_t i = 0; i < kWaitLimit; ++i) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if ((i & 1023u) == 1023u && global_ns() - t0 > limit_ns) break;
-    }
-    return false;
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
-                 "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-// This thread's bulk stores have finished reading shared memory / are complete.
-__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t fold4(uint32_t i) { return ((i >> 4) ^ (i >> 8) ^ (i >> 12)) & 15u; }
 
@@ -350,83 +295,6 @@ __device__ __forceinline__ void op_dense5(float2 (&v)[NR], const float2* __restr
 // apart (SBO).  B is K-major without swizzle: 8 x 16 B core matrices,
 // LBO = 128 B between the K chunks of one row group, SBO = 1024 B between
 // 8-row groups.  D column n of row t is read back by thread t.
-constexpr uint32_t kTcCols = 256;               // per M-block: D1 (64 columns) | D2 (64 columns)
-constexpr uint32_t kTcBBytes = 16384;          // B hi (8 KB) + B lo (8 KB)
-constexpr uint32_t kTcIdescBase = (1u << 4)    // D format F32
-                                  | (1u << 7)  // A format BF16
-                                  | (1u << 10) // B format BF16
-                                  | ((128u >> 4) << 24);  // M = 128
-constexpr uint32_t kTcIdesc64 = kTcIdescBase | ((64u >> 3) << 17);     // N = 64
-constexpr uint32_t kTcIdesc128 = kTcIdescBase | ((128u >> 3) << 17);   // N = 128  // M = 128
-
-// B: no swizzle, LBO 128 B, SBO 1024 B.
-__device__ __forceinline__ uint64_t umma_desc_b(uint32_t smem_addr) {
-    return static_cast<uint64_t>((smem_addr >> 4) & 0x3FFFu) | (static_cast<uint64_t>(128u >> 4) << 16) |
-           (static_cast<uint64_t>(1024u >> 4) << 32) | (uint64_t{1} << 46);
-}
-// A: 128-byte swizzle (layout code 2), SBO 1024 B (LBO unused: K fits one
-// swizzle row).  K steps advance the start address by 32 B inside the
-// 1024-byte-aligned swizzle atom.
-__device__ __forceinline__ uint64_t umma_desc_a(uint32_t smem_addr) {
-    return static_cast<uint64_t>((smem_addr >> 4) & 0x3FFFu) | (uint64_t{1} << 16) |
-           (static_cast<uint64_t>(1024u >> 4) << 32) | (uint64_t{1} << 46) | (uint64_t{2} << 61);
-}
-
-__device__ __forceinline__ float bf16_to_float(uint32_t b) { return __uint_as_float(b << 16); }
-
-// (re, im) -> hi = bf16x2(re, im), lo = bf16x2 of the residuals (re in the low half).
-__device__ __forceinline__ void tc_split(float2 x, uint32_t& hi, uint32_t& lo) {
-    const __nv_bfloat162 h = __floats2bfloat162_rn(x.x, x.y);
-    const uint32_t hb = *reinterpret_cast<const uint32_t*>(&h);
-    const float2 r = __fadd2_rn(x, make_float2(-bf16_to_float(hb & 0xFFFFu), -__uint_as_float(hb & 0xFFFF0000u)));
-    const __nv_bfloat162 l = __floats2bfloat162_rn(r.x, r.y);
-    hi = hb;
-    lo = *reinterpret_cast<const uint32_t*>(&l);
-}
-
-// Writes this thread's row of A (hi and lo), kappa = identity: chunk j holds
-// amplitudes 4j .. 4j+3.
-__device__ __forceinline__ void tc_write_a(const float2 (&v)[NR], unsigned char* a_hi, unsigned char* a_lo) {
-    const uint32_t t = threadIdx.x;
-#pragma unroll
-    for (uint32_t j = 0; j < 8; ++j) {
-        uint32_t hi[4], lo[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) tc_split(v[4 * j + e], hi[e], lo[e]);
-        const uint32_t off = t * 128u + ((j ^ (t & 7u)) << 4);
-        *reinterpret_cast<uint4*>(a_hi + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-        *reinterpret_cast<uint4*>(a_lo + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-    }
-}
-
-__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-        ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
-        : "memory");
-}
-__device__ __forceinline__ void tc_commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-__device__ __forceinline__ void tc_ld_32(uint32_t taddr, uint32_t (&r)[32]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr)
-        : "memory");
-}
-
 struct TcCtx {
     uint32_t tmem;        // TMEM base address (lane 0, column base)
     uint64_t* bar;        // MMA-completion mbarrier
@@ -1137,6 +1005,8 @@ void launch_tile_kernel(unsigned grid, const TileWork& single, const TileWork* w
 cudaError_t launch_tile_pass(float2* state, uint32_t n, const TilePass* d_passes, const TilePhase* d_phases,
                              const TileOp* d_ops, const float2* d_mats, uint32_t pass_index, int features,
                              int* err, cudaStream_t s) {
+    if (features & kPassChain)
+        return launch_chain_pass(state, n, d_passes, d_phases, d_ops, d_mats, pass_index, err, s);
     cudaError_t e = configure_tile_kernel();
     if (e != cudaSuccess) return e;
     const uint64_t tiles = uint64_t{1} << (n - kTileQubits);

@@ -171,6 +171,10 @@ constexpr int kPassWide = 2;
 constexpr int kPassSwaps = 4;
 constexpr int kPassPairs = 8;
 constexpr int kPassCtl = 16;
+// The pass is in chain form (every register phase one tensor-core op): a
+// single-state launch runs it on the tensor-core chain kernel (chain.cu).
+// Not a body feature: tile_body() ignores it.
+constexpr int kPassChain = 32;
 
 // Kernel bodies (instantiations of the tile kernel), smallest first: 1-qubit,
 // controlled and diagonal ops; those plus register SWAPs; uncontrolled
@@ -204,6 +208,12 @@ cudaError_t launch_tile_pass(float2* state, uint32_t n, const TilePass* d_passes
                              const TileOp* d_ops, const float2* d_mats, uint32_t pass_index, int features,
                              int* err, cudaStream_t s);
 int sm_count();   // multiprocessors of the current device (cached)
+
+// The chain kernel (chain.cu): one launch applies chain pass `pass_index`
+// to the state; returns the launch status.
+cudaError_t launch_chain_pass(float2* state, uint32_t n, const TilePass* d_passes, const TilePhase* d_phases,
+                              const TileOp* d_ops, const float2* d_mats, uint32_t pass_index, int* err,
+                              cudaStream_t s);
 
 // Runs the tile kernel's bounded mbarrier wait on a barrier that never
 // completes; *err becomes 1 when the wait gives up (as it must).

@@ -11,6 +11,7 @@ import numpy as np
 TOP_U1, TOP_X, TOP_SWAP, TOP_U2, TOP_DENSE, TOP_U1R, TOP_RX, TOP_CPHASE, TOP_DENSE_TC = range(1, 10)
 TOP_DIAG = 11
 STEP_PASS, STEP_PLAIN, STEP_MEASURE, STEP_SWAP = range(4)
+PASS_CHAIN = 32
 
 
 def apply_k(st, n, qubits, mat, ctrl_mask=0):
@@ -40,6 +41,9 @@ def emulate(plan, init=None):
     mats = m2[:, 0] + 1j * m2[:, 1] if len(m2) else np.zeros(0, dtype=np.complex128)
     for step in plan["steps"]:
         kind = step["kind"]
+        if kind == STEP_PASS and plan["passes"][step["index"]]["features"] & PASS_CHAIN:
+            emulate_chain_pass(plan, plan["passes"][step["index"]], st, n)
+            continue
         if kind == STEP_PASS:
             P = plan["passes"][step["index"]]
             tp = P["tile_pos"]
@@ -184,3 +188,79 @@ def decode_tc_flat(plan, data, flags=None):
         kap = np.array([sum(((c >> j) & 1) << perm[j] for j in range(5)) for c in range(32)])
         _tc_cache[key] = B[0::2][:, 2 * kap] + 1j * B[1::2][:, 2 * kap]
     return _tc_cache[key]
+
+
+def _tc_w(plan, data):
+    """W[r][kap]: the complex matrix a tensor-core op's B image applies to
+    the A row's amplitudes in K (kappa) order."""
+    flat = np.array(plan["mats"], dtype=np.uint32)
+    raw = flat[2 * data:2 * data + 4096].tobytes()
+    u16 = np.frombuffer(raw, dtype=np.uint16).astype(np.uint32)
+    nn = np.arange(64)[:, None]
+    kk = np.arange(64)[None, :]
+    at = (nn // 8) * 1024 + (kk // 8) * 128 + (nn % 8) * 16 + (kk % 8) * 2
+    hi = (u16[at // 2] << 16).astype(np.uint32).view(np.float32).astype(np.float64)
+    lo = (u16[(8192 + at) // 2] << 16).astype(np.uint32).view(np.float32).astype(np.float64)
+    B = hi + lo
+    return B[0::2][:, 0::2] + 1j * B[1::2][:, 0::2]
+
+
+def _bits_or(idx, positions):
+    """OR over the set bits j of idx of (1 << positions[j])."""
+    out = np.zeros(np.shape(idx), dtype=np.int64)
+    for j, p in enumerate(positions):
+        out |= ((idx >> j) & 1) << int(p)
+    return out
+
+
+def _bits_xor(idx, values):
+    out = np.zeros(np.shape(idx), dtype=np.int64)
+    for j, v in enumerate(values):
+        out ^= ((idx >> j) & 1) * int(v)
+    return out
+
+
+def emulate_chain_pass(plan, P, st, n):
+    """The tensor-core chain kernel (chain.cu) replayed at byte level: the
+    tile is read in phase 0's layout, scattered into the first op's A
+    operand (own rows when phase 0 holds the op, else the entry offsets),
+    multiplied by the op's B image, read back row by row and scattered into
+    the next op's A by that phase's XOR offsets, and after the last op
+    stored from the last phase's layout."""
+    tp = P["tile_pos"]
+    phases = P["phases"]
+    first = 0 if phases[0]["ops"] else 1
+    last = len(phases) - 1 if phases[-1]["ops"] else len(phases) - 2
+    tile_set = set(tp)
+    out_mem = [q for q in range(n) if q not in tile_set]
+    t = np.arange(256, dtype=np.int64)[:, None]
+    r = np.arange(32, dtype=np.int64)[None, :]
+    R = phases[0]
+    read_l = _bits_or(t, [R["thr_pos"][j] for j in range(8)]) | _bits_or(r, [R["reg_pos"][j] for j in range(5)])
+    if first == 0:
+        off0 = 128 * t + (((r // 4) ^ (t & 7)) << 4) + 4 * (r % 4)
+    else:
+        F = phases[first]
+        off0 = _bits_xor(t, F["a_thr"]) ^ _bits_xor(r, F["a_reg"])
+    l_all = np.arange(8192, dtype=np.int64)
+    mem_l = _bits_or(l_all, tp)
+    for tile in range(1 << (n - 13)):
+        base = int(_bits_or(np.array(tile, dtype=np.int64), out_mem))
+        buf = st[base | mem_l]
+        v = buf[read_l]                              # (256, 32): thread t, register r
+        off = off0
+        for oi in range(first, last + 1):
+            assert np.all(off % 4 == 0) and np.all(off < 32768) and np.unique(off).size == 8192
+            row = off // 128
+            chunk = ((off % 128) // 16) ^ (row & 7)
+            kap = chunk * 4 + (off % 16) // 4
+            A = np.zeros((256, 32), dtype=np.complex128)
+            A[row, kap] = v
+            W = _tc_w(plan, phases[oi]["ops"][0]["data"])
+            v = A @ W.T                               # D row t, register r (phase oi's layout)
+            if oi < last:
+                F = phases[oi + 1]
+                off = _bits_xor(t, F["a_thr"]) ^ _bits_xor(r, F["a_reg"])
+        L = phases[last]
+        g = base | _bits_or(t, [tp[p] for p in L["thr_pos"]]) | _bits_or(r, [tp[p] for p in L["reg_pos"]])
+        st[g] = v

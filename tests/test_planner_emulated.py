@@ -112,3 +112,20 @@ def test_tensor_core_phase_entry_offsets(n, depth, seed):
                     seen.add(off)
             assert len(seen) == 8192 and max(seen) < 32768
     assert entries > 0
+
+
+@pytest.mark.parametrize("n,depth", [(14, 12), (16, 24)])
+def test_chain_passes_of_the_fused_rotation_circuit(n, depth):
+    """The benchmarked form (k <= 5 fusion + windowing) in tensor-core mode:
+    most passes are chain passes (phases of one tensor-core op each), which
+    the emulator replays with the chain kernel's byte-level data movement."""
+    from qlassical_b200.middleware import Middleware, TranspilerConfig
+    m = circuits.random_rot_cz(n, depth, seed=1234)
+    f = Middleware().transpile(m, config=TranspilerConfig(max_fusion_qubits=5))
+    plan = describe_plan(f, n, "tiled_tc")
+    chain = sum(1 for P in plan["passes"] if P["features"] & 32)
+    assert chain >= 1 and plan["stats"]["chain_passes"] == chain
+    want, _ = oracle.run_oracle(m)
+    got = emulate(plan)
+    assert oracle.max_abs_diff(want, got) < TOL["tiled_tc"]
+    assert oracle.infidelity(want, got) < 1e-6
