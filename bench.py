@@ -12,6 +12,9 @@ loop, bench_hw_awareness.cpp:102-107).  amp-updates = gates x 2^n
 carries the same blocks on FP32 CUDA cores, the unfused circuit on the FP32
 tile path, one sweep per instruction, and a sampled-amplitude comparison of
 the tensor-core result with the unfused FP32 result.
+The default line also carries, under "configs", the 33-qubit QFT, the
+batched mode (4096 HEA circuits) and the serving loop (Poisson arrivals),
+each with its own roofline, clocks and accuracy check.
   python bench.py --circuit rot_cz | qft               the unfused circuit / the QFT (tiled)
 
   python bench.py [--gpus N --steps K --warmup W]      our engine (N replicas)
@@ -62,6 +65,8 @@ def parse():
                     help="plain | tiled | tiled_tc (default: tiled_tc for the fused circuit, tiled otherwise)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the QFT, batched and serving sub-runs of the default line")
     ap.add_argument("--workload", default="circuit", choices=["circuit", "batched", "serving"])
     ap.add_argument("--circuit", default="fused", choices=["fused", "rot_cz", "qft"],
                     help="circuit workload: the rotation + CZ circuit after k<=5 fusion and windowing (default), "
@@ -493,12 +498,37 @@ def run_ours(args):
         except Exception as ex:  # the oracle libraries are test infrastructure
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
                                     "sample": f"unavailable: {ex}"}
-    if rank == 0:
-        print(json.dumps(line))
     del plan
     del eng
+    if rank == 0 and world == 1 and not args.no_configs and args.circuit == "fused":
+        # The other configurations, each with its own roofline, clocks and
+        # accuracy check: the 33-qubit QFT (68.7 GB), the batched mode and
+        # the serving loop.
+        configs = {}
+        free = _free_device_bytes(q)
+        nq = 33 if free >= (1 << 33) * 8 + (8 << 30) else 32
+        for key, fn in (("qft", lambda: qft_workload(q, nq)),
+                        ("batched", lambda: batched_workload(q, args)),
+                        ("serving", lambda: serving_workload(q, args))):
+            t0 = time.perf_counter()
+            try:
+                configs[key] = fn()
+            except Exception as ex:     # reported, never hidden
+                configs[key] = {"error": f"{type(ex).__name__}: {ex}"}
+            configs[key]["wall_s"] = time.perf_counter() - t0
+        line["configs"] = configs
+    if rank == 0:
+        print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
+
+
+def _free_device_bytes(q):
+    import ctypes
+    from qlassical_b200 import _lib
+    free, total, sm = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_int()
+    _lib.call("qlb_device_info", ctypes.byref(sm), ctypes.byref(free), ctypes.byref(total))
+    return free.value
 
 
 def _peak_hbm():
@@ -516,23 +546,18 @@ def _peak_source():
     return "fallback 6650 GB/s (MEASURED_PEAKS.json absent)"
 
 
-def run_batched(args):
+def batched_workload(q, args, rank=0, world=1, mode="auto"):
     """Batched workload: `--circuits` HEA circuits (n log-uniform in [10, 20],
     depth U{8..32}); a step = one run of the whole batch (|0...0> set-up, all
-    circuits, FP64 <Z_i>, results to pinned host memory) as one graph launch."""
+    circuits, FP64 <Z_i>, results to pinned host memory) as one graph launch.
+    Beside it: sequential plain launches measured on the first 256 circuits,
+    and the FP64 <Z_i> checked against the oracle on the first 64."""
     import numpy as np
     import torch
-    from __graft_entry__ import package
-    q = package()
     from qlassical_b200 import circuits
     from qlassical_b200.batch import Batch
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    torch.cuda.set_device(local)
-    q.engine.set_device(local)
     mods = circuits.hea_batch(args.circuits, seed=2024)
-    mode = args.mode if args.mode in ("tiled", "tiled_tc", "auto") else "tiled"
     t0 = time.perf_counter()
     b = Batch(mods, mode)
     build_s = time.perf_counter() - t0
@@ -541,16 +566,17 @@ def run_batched(args):
     for _ in range(args.warmup):
         b.run()
     b.synchronize()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    steps = max(3, args.steps)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     with ClockSampler(local) as clk:
-        for i in range(args.steps):
+        for i in range(steps):
             starts[i].record(stream)
             b.run()
             ends[i].record(stream)
         b.synchronize()
     total_ms = sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends))
-    step_s = total_ms / 1e3 / args.steps
+    step_s = total_ms / 1e3 / steps
     value = world * len(mods) / step_s
     ez = b.expect_z()
     del b
@@ -562,7 +588,7 @@ def run_batched(args):
     ez2 = run_batch(mods, mode)
     e2e_s = time.perf_counter() - t0
     assert all(np.array_equal(x, y) for x, y in zip(ez, ez2))
-    # sequential plain launches: one engine per size, one circuit at a time
+    # sequential plain launches, measured: one engine per size, one circuit at a time
     sample = mods[:256]
     engines = {}
     t0 = time.perf_counter()
@@ -575,29 +601,37 @@ def run_batched(args):
         eng.expect_z()
     seq_plain = len(sample) / (time.perf_counter() - t0)
     engines.clear()
+    # accuracy: FP64 <Z_i> of the first 64 circuits against the oracle
+    from oracle import oracle
+    worst = 0.0
+    for m, z in zip(mods[:64], ez[:64]):
+        ref, _ = oracle.run_oracle(m)
+        worst = max(worst, float(np.max(np.abs(circuits.expect_z_of(ref, m.num_qubits) - z))))
     # roofline: every tile pass reads and writes 16 B per amplitude
     bytes_step = st["tiles"] * 8192 * 16.0
     achieved = bytes_step / step_s / 1e9
     peak = _peak_hbm()
     line = {
-        "metric": "circuits/s", "value": value, "unit": "circuits/s", "n_gpus": world, "steps": args.steps,
+        "metric": "circuits/s", "value": value, "unit": "circuits/s", "n_gpus": world, "steps": steps,
         "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64 (fp32)", "data": "synthetic",
         "config": {"workload": f"{len(mods)} HEA circuits (RY,RZ per qubit + CZ ladder), n log-uniform in "
                                f"[10, 20], depth U{{8..32}}, <Z_i> per circuit",
                    "circuits": len(mods), "mode": st["mode"], "rounds": st["rounds"], "passes": st["passes"],
                    "amp_updates_per_step": st["amp_updates"], "state_bytes": st["state_bytes"],
-                   "build_s": build_s, "l2": "4 GB of states, larger than the 126 MB L2"},
+                   "autotune_ms": list(st["autotune_ms"]), "build_s": build_s,
+                   "l2": "4 GB of states, larger than the 126 MB L2"},
         "amp_updates_per_s": st["amp_updates"] / step_s,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": TRAFFIC_PER_ALGORITHMIC_BYTE * bytes_step / max(1, st["rounds"]),
                      "traffic_source": "ncu dram bytes of a 26-qubit pass, scaled to the tiles of a round",
-                     "kernel": "k_tile_pass (all rounds)",
-                     "peak_source": _peak_source()},
+                     "kernel": "k_tile_pass (all rounds)", "peak_source": _peak_source()},
         "sequential_plain": {"value": seq_plain, "unit": "circuits/s",
-                             "sample": "first 256 circuits, CUDAEngine plain mode, one circuit at a time"},
+                             "sample": "first 256 circuits, CUDAEngine plain mode, one circuit at a time (measured)"},
+        "accuracy_check": {"vs": "oracle (complex128 host state) <Z_i>, first 64 circuits",
+                           "max_abs_diff_expect_z": worst, "tolerance": 2e-5},
         "clocks": clk.summary(),
-        "gpu_launches": args.steps * st["launches"],
+        "gpu_launches": steps * st["launches"],
         "e2e": {"value": len(mods) / e2e_s, "unit": "circuits/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
     }
@@ -618,24 +652,35 @@ def run_batched(args):
         except Exception as ex:
             line["cpu_baseline"] = {"value": None, "unit": "circuits/s", "cores": None, "kind": "reference",
                                     "sample": f"unavailable: {ex}"}
+    return line
+
+
+def run_batched(args):
+    import torch
+    from __graft_entry__ import package
+    q = package()
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    q.engine.set_device(local)
+    mode = args.mode if args.mode in ("tiled", "tiled_tc", "auto") else "auto"
+    line = batched_workload(q, args, rank, world, mode)
     if rank == 0:
         print(json.dumps(line))
 
 
-def run_serving(args):
+def serving_workload(q, args):
     """Serving workload: `--requests` requests (random_h_rx_cx recipe, n
     log-uniform in [12, 30], depth U{10..40}, 1024 shots + <Z_i> each)
-    arriving as a Poisson process of rate `--rate`; latency = finish - submit."""
+    arriving as a Poisson process of rate `--rate`; latency = finish - submit.
+    The sequential-plain baseline is measured: every request runs alone
+    through CUDAEngine(mode="plain") (execute, <Z_i>, 1024 samples), and the
+    same arrivals are queued one request at a time on those service times."""
     import numpy as np
-    import torch
-    from __graft_entry__ import package
-    q = package()
     from qlassical_b200 import circuits
     from qlassical_b200.serve import Server
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    rank = int(os.environ.get("RANK", "0"))
-    torch.cuda.set_device(local)
-    q.engine.set_device(local)
     mods = circuits.serving_requests(args.requests, seed=7)
     arrivals = circuits.poisson_arrivals(args.requests, args.rate, seed=11)
     srv = Server()
@@ -652,40 +697,55 @@ def run_serving(args):
             ids[i] = srv.submit(m, shots=1024, seed=i)
         res = [srv.result(i) for i in ids]
     stats = srv.stats()
+    # alone vs in the mix: two small requests again, each alone in the server
+    small = [i for i, m in enumerate(mods) if m.num_qubits <= 16][:2]
+    same = True
+    for i in small:
+        r = srv.result(srv.submit(mods[i], shots=1024, seed=i))
+        same = same and np.array_equal(r.expect_z, res[i].expect_z) and np.array_equal(r.samples, res[i].samples)
     srv.close()
     lat = np.array([r.latency for r in res])
     ns = np.array([m.num_qubits for m in mods])
     span = max(r.t_done for r in res) - min(r.t_submit for r in res)
     gates = np.array([m.gate_count() for m in mods], dtype=np.float64)
     amp_updates = float(np.sum(gates * np.exp2(ns)))
-    # sequential plain launches: service time per request from plain-mode
-    # rates measured at two sizes, queued one at a time on the same arrivals
-    rates = {}
-    for n_probe in (16, 24):
-        m = circuits.random_h_rx_cx(n_probe, 10, seed=3)
-        eng = q.CUDAEngine(n_probe, mode="plain")
-        eng.execute(m)
+    # accuracy: <Z_i> of the requests of <= 16 qubits against the oracle
+    from oracle import oracle
+    worst = 0.0
+    for i, m in enumerate(mods):
+        if m.num_qubits <= 16:
+            ref, _ = oracle.run_oracle(m)
+            worst = max(worst, float(np.max(np.abs(circuits.expect_z_of(ref, m.num_qubits) - res[i].expect_z))))
+    # sequential plain launches, measured: each request alone, then queued FIFO on the same arrivals
+    engines = {}
+    svc = []
+    for m in mods:
+        eng = engines.get(m.num_qubits)
+        if eng is None:
+            for k in [k for k in engines if k >= 27]:   # keep at most one large state resident
+                del engines[k]
+            eng = engines[m.num_qubits] = q.CUDAEngine(m.num_qubits, mode="plain")
         eng.synchronize()
         t_ = time.perf_counter()
         eng.reset()
         eng.execute(m)
         eng.expect_z()
         eng.sample(1, 1024)
-        rates[n_probe] = m.gate_count() * float(1 << n_probe) / (time.perf_counter() - t_)
-        del eng
+        svc.append(time.perf_counter() - t_)
+    engines.clear()
     done = 0.0
     seq_lat = []
-    for i, m in enumerate(mods):
-        rate = rates[16] if m.num_qubits < 20 else rates[24]
-        svc = m.gate_count() * float(1 << m.num_qubits) / rate
+    for i in range(len(mods)):
         start = max(arrivals[i], done)
-        done = start + svc
+        done = start + svc[i]
         seq_lat.append(done - arrivals[i])
     seq_lat = np.array(seq_lat)
     h2d = sum(m.program().nbytes for m in mods)
     d2h = sum(8 * m.num_qubits + 8 * 1024 for m in mods)
     p99 = float(np.percentile(lat, 99))
-    line = {
+    hbm = stats["tiles"] * 8192 * 16.0 / span / 1e9
+    peak = _peak_hbm()
+    return {
         "metric": "request latency p99", "value": p99, "unit": "s", "n_gpus": 1, "steps": len(mods),
         "warmup": 4, "ms_per_step": 1e3 * span / len(mods), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64 (fp32)", "data": "synthetic",
@@ -697,17 +757,111 @@ def run_serving(args):
         "p50_large_s": float(np.percentile(lat[ns >= 22], 50)) if np.any(ns >= 22) else None,
         "circuits_per_s": len(mods) / span, "amp_updates_per_s": amp_updates / span,
         "server": stats,
+        "roofline": {"bound": "hbm", "achieved": hbm, "peak": peak, "unit": "GB/s", "frac": hbm / peak,
+                     "of": "tile-pass bytes (16 B per amplitude per pass) over the whole span, idle time included",
+                     "kernel": "k_tile_pass (all rounds)", "peak_source": _peak_source()},
         "sequential_plain": {"p50_s": float(np.percentile(seq_lat, 50)), "p99_s": float(np.percentile(seq_lat, 99)),
                              "circuits_per_s": len(mods) / max(1e-9, done - arrivals[0]),
-                             "method": "plain-mode service times from rates measured at 16 and 24 qubits, "
-                                       "queued one request at a time on the same arrivals (modelled)"},
+                             "service_s_total": float(sum(svc)),
+                             "method": "measured: every request run alone through CUDAEngine(mode='plain') "
+                                       "(execute, <Z_i>, 1024 samples), queued FIFO on the same arrival times"},
+        "accuracy_check": {"vs": "oracle (complex128 host state) <Z_i>, requests of <= 16 qubits",
+                           "max_abs_diff_expect_z": worst, "tolerance": 2e-5,
+                           "alone_equals_mix": bool(same), "alone_checked": len(small)},
         "clocks": clk.summary(),
         "gpu_launches": int(stats["launches"]),
         "e2e": {"value": p99, "unit": "s", "h2d_bytes_per_step": int(h2d / len(mods)),
                 "d2h_bytes_per_step": int(d2h / len(mods))},
     }
+
+
+def run_serving(args):
+    import torch
+    from __graft_entry__ import package
+    q = package()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    q.engine.set_device(local)
+    line = serving_workload(q, args)
     if rank == 0:
         print(json.dumps(line))
+
+
+def qft_workload(q, n):
+    """The QFT of |0...0> at n qubits (68.7 GB at 33): the unfused circuit on
+    the tile path (diagonal terms deferred; the engine's fastest form), its
+    passes' HBM roofline, and beside it the middle end's fusion into blocks
+    of up to 6 qubits and of up to 5 qubits (tensor cores) and one sweep
+    per instruction, each checked against the analytic QFT|0> (all
+    amplitudes 2^(-n/2)) on 65,536 sampled amplitudes."""
+    import numpy as np
+    import torch
+    from qlassical_b200 import circuits
+    from qlassical_b200.middleware import Middleware, TranspilerConfig
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    module = circuits.qft(n)
+    gates = module.gate_count()
+    amp = gates * float(1 << n)
+    eng = q.CUDAEngine(n, mode="tiled")
+    stream = torch.cuda.ExternalStream(eng.stream())
+    rng = np.random.default_rng(5)
+    idx = rng.integers(0, 1 << n, size=1 << 16, dtype=np.uint64)
+    exact = 1.0 / math.sqrt(float(1 << n))
+
+    def accuracy():
+        got = eng.amplitudes_at(idx)
+        return {"max_abs_diff": float(np.max(np.abs(got - exact))),
+                "sampled_infidelity": float(1.0 - abs(np.sum(got) * exact) ** 2 /
+                                            (idx.size * exact * exact * np.vdot(got, got).real))}
+
+    def timed(mod, mode, reps=1):
+        eng.set_mode(mode)
+        p = eng.compile(mod)
+        eng.reset()
+        eng.run(p)
+        ms = []
+        for _ in range(reps):
+            eng.reset()
+            eng.synchronize()
+            s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s_.record(stream)
+            eng.run(p)
+            e_.record(stream)
+            eng.synchronize()
+            ms.append(s_.elapsed_time(e_))
+        st_ = p.stats()
+        del p
+        return statistics.median(ms), st_
+
+    with ClockSampler(local) as clk:
+        ms, st = timed(module, "tiled", reps=3)
+    acc = accuracy()
+    per_pass = ms / max(1, st["launches"])
+    achieved = 16.0 * float(1 << n) / (per_pass / 1e3) / 1e9
+    peak = _peak_hbm()
+    forms = {}
+    for k, key, mode in ((6, "fused_k6", "tiled_tc"), (5, "fused_k5_tensor_cores", "tiled_tc")):
+        fm = Middleware().transpile(circuits.qft(n), config=TranspilerConfig(max_fusion_qubits=k))
+        fms, fst = timed(fm, mode)
+        forms[key] = {"value": amp / (fms / 1e3), "ms": fms, "tile_passes": fst["tile_passes"],
+                      "sweeps": fst["sweeps"], "tc_ops": fst["tc_ops"], **accuracy()}
+    pms, pst = timed(module, "plain")
+    forms["plain_gpu"] = {"value": amp / (pms / 1e3), "ms": pms, "sweeps": pst["sweeps"], **accuracy()}
+    del eng
+    return {
+        "metric": METRIC, "value": amp / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "dtype": "c64 (fp32)",
+        "config": {"workload": f"QFT (H + CP ladders + bit-reversal swaps) of |0...0>, {n} qubits",
+                   "n_qubits": n, "gates": gates, "state_bytes": (1 << n) * 8, "mode": "tiled",
+                   "passes": st["tile_passes"], "launches": st["launches"]},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": TRAFFIC_PER_ALGORITHMIC_BYTE * 16.0 * float(1 << n),
+                     "kernel": "k_tile_pass", "peak_source": _peak_source()},
+        "accuracy_check": {"vs": "analytic QFT|0> (every amplitude 2^(-n/2)), 65,536 sampled amplitudes",
+                           "tolerance": {"sampled_infidelity": 1e-6}, **acc},
+        "comparisons": forms,
+        "clocks": clk.summary(),
+    }
 
 
 def main():
