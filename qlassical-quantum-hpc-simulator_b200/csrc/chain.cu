@@ -210,8 +210,12 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                 }
                 if (lane != 0) mbar_arrive(&full[b]);
             } else {
+                // g: memory index (its tile bits start at zero, so XOR sets
+                // them); d: byte offset inside the buffer (XOR-ed likewise),
+                // added to the buffer's shared address at each copy
                 uint64_t g = base | gl;
-                uint32_t d = smem_u32(dst) + 16u * lane;
+                const uint32_t dbase = smem_u32(dst);
+                uint32_t d = 16u * lane;
                 // pieces in Gray-code order of c: one address bit changes per
                 // step (bits 0..2 inside a group of 8, bits 3..6 between groups)
 #pragma unroll 1
@@ -228,7 +232,8 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                             g ^= hb[bit];
                             d ^= 512u << bit;
                         }
-                        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(state + g) : "memory");
+                        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dbase + d), "l"(state + g)
+                                     : "memory");
                     }
                     // back to lo = 0 of this group's Gray sequence: 0,1,3,2,6,7,5,4 ends at 4
                     g ^= hb[2];

@@ -129,3 +129,37 @@ def test_chain_passes_of_the_fused_rotation_circuit(n, depth):
     got = emulate(plan)
     assert oracle.max_abs_diff(want, got) < TOL["tiled_tc"]
     assert oracle.infidelity(want, got) < 1e-6
+
+
+def test_chain_load_warp_addressing():
+    """The chain kernel's load warp walks its 128 16-byte pieces per lane in
+    Gray-code order, XOR-ing one memory bit and one buffer-offset bit per
+    step (chain.cu).  Replayed here: every piece of the 64 KB buffer is
+    written exactly once, at an offset inside the buffer, from the memory
+    index its tile-local index maps to."""
+    rng = np.random.default_rng(3)
+    for _ in range(4):
+        tp = [0, 1, 2] + sorted(int(x) for x in rng.choice(np.arange(3, 30), 10, replace=False))
+        mem_of = lambda l: sum(1 << tp[j] for j in range(13) if (l >> j) & 1)   # noqa: E731
+        hb = [1 << tp[6 + i] for i in range(7)]
+        seen = {}
+        for lane in range(32):
+            gl = sum(1 << tp[1 + i] for i in range(5) if (lane >> i) & 1)
+            g, d = gl, 16 * lane
+            for hi in range(16):
+                if hi:
+                    bit = (hi & -hi).bit_length() - 1
+                    g ^= hb[3 + bit]
+                    d ^= 4096 << bit
+                for lo in range(8):
+                    if lo:
+                        bit = 0 if lo & 1 else (1 if lo & 2 else 2)
+                        g ^= hb[bit]
+                        d ^= 512 << bit
+                    assert 0 <= d < 65536 and d % 16 == 0 and d not in seen
+                    seen[d] = g
+                g ^= hb[2]
+                d ^= 2048
+        assert len(seen) == 4096
+        for d, g in seen.items():
+            assert g == mem_of(d // 8)
