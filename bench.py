@@ -65,6 +65,8 @@ def parse():
                     help="plain | tiled | tiled_tc (default: tiled_tc for the fused circuit, tiled otherwise)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-chain", action="store_true",
+                    help="run every pass on the general tile kernel (QLB_OPT_TC_CHAIN = 0)")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the QFT, batched and serving sub-runs of the default line")
     ap.add_argument("--workload", default="circuit", choices=["circuit", "batched", "serving"])
@@ -309,6 +311,8 @@ def run_ours(args):
     n = module.num_qubits
     gates = logical_gates(args, module)
     eng = q.CUDAEngine(n, seed=1, mode=args.mode)
+    if args.no_chain:
+        eng.set_option(3, 0)     # QLB_OPT_TC_CHAIN
     plan = eng.compile(module)
     pstats = plan.stats()
     stream = torch.cuda.ExternalStream(eng.stream())
@@ -380,6 +384,7 @@ def run_ours(args):
     e2e_value = world * amp_updates_step / e2e_t
 
     extra = {"mode": args.mode, "passes_per_step": passes, "launches_per_step": pstats["launches"],
+             "chain_passes_per_step": pstats.get("chain_passes", 0),
              "parallelism": f"replicas x{world}"}
     plain = None
     comparisons = {}
