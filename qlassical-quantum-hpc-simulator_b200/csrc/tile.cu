@@ -1005,8 +1005,6 @@ void launch_tile_kernel(unsigned grid, const TileWork& single, const TileWork* w
 cudaError_t launch_tile_pass(float2* state, uint32_t n, const TilePass* d_passes, const TilePhase* d_phases,
                              const TileOp* d_ops, const float2* d_mats, uint32_t pass_index, int features,
                              int* err, cudaStream_t s) {
-    if (features & kPassChain)
-        return launch_chain_pass(state, n, d_passes, d_phases, d_ops, d_mats, pass_index, err, s);
     cudaError_t e = configure_tile_kernel();
     if (e != cudaSuccess) return e;
     const uint64_t tiles = uint64_t{1} << (n - kTileQubits);

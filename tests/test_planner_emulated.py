@@ -163,3 +163,70 @@ def test_chain_load_warp_addressing():
         assert len(seen) == 4096
         for d, g in seen.items():
             assert g == mem_of(d // 8)
+
+
+def _chain_geometry(tp, n):
+    """chain.cu's chain_tensor_map(): dimensions at the tile's runs of
+    consecutive memory qubits (at most 8 long), the first five boxed, the
+    rest enumerated by copies."""
+    runs, i = [], 0
+    while i < 13:
+        ln = 1
+        while i + ln < 13 and ln < 8 and tp[i + ln] == tp[i] + ln:
+            ln += 1
+        runs.append((tp[i], ln))
+        i += ln
+    nd = min(len(runs), 5)
+    lo = [runs[d][0] if d < nd else 64 for d in range(5)]
+    dims, box, strides = [], [], []
+    for d in range(5):
+        if d < nd:
+            hi = runs[d + 1][0] if d + 1 < nd else n
+            dims.append(1 << (hi - runs[d][0]))
+            box.append(1 << runs[d][1])
+        else:
+            dims.append(1)
+            box.append(1)
+        if d > 0:
+            strides.append(8 << runs[d][0] if d < nd else 8 << n)
+    rem = [runs[r][0] + k for r in range(nd, len(runs)) for k in range(runs[r][1])]
+    boxed = sum(runs[d][1] for d in range(nd))
+    return lo, dims, box, strides, rem, 8 << boxed
+
+
+def test_chain_tma_geometry():
+    """Every TMA box of every tile lands its amplitudes at their tile-order
+    offsets, inside the tensor and the 64 KB buffer, with 16-byte-aligned
+    starts (chain.cu: chain_tensor_map, tile_coords)."""
+    rng = np.random.default_rng(11)
+    for n in (14, 17, 20, 30, 34):
+        for _ in range(6):
+            others = sorted(int(x) for x in rng.choice(np.arange(3, n), 10, replace=False))
+            tp = [0, 1, 2] + others
+            lo, dims, box, strides, rem, box_bytes = _chain_geometry(tp, n)
+            out = [q for q in range(n) if q not in tp]
+            assert box_bytes * (1 << len(rem)) == 65536 and box[0] * 8 % 16 == 0
+            assert all(st % 16 == 0 and st < 2 ** 40 for st in strides)
+            assert all(b <= 256 and b <= dm for b, dm in zip(box, dims)) and all(dm < 2 ** 32 for dm in dims)
+            mem_of = lambda l: sum(1 << tp[j] for j in range(13) if (l >> j) & 1)   # noqa: E731
+            for tile in [0, 1, (1 << (n - 13)) - 1, int(rng.integers(0, 1 << (n - 13)))]:
+                base = sum(1 << out[j] for j in range(len(out)) if (tile >> j) & 1)
+                for cpy in range(1 << len(rem)):
+                    c = [0] * 5
+                    for j, q in enumerate(out):
+                        if (tile >> j) & 1:
+                            d = max(k for k in range(5) if lo[k] <= q)
+                            c[d] |= 1 << (q - lo[d])
+                    for i, q in enumerate(rem):
+                        if (cpy >> i) & 1:
+                            c[4] |= 1 << (q - lo[4])
+                    assert all(c[d] + box[d] <= dims[d] for d in range(5)) and (c[0] * 8) % 16 == 0
+                    # box element (i0..i4) -> tensor element -> memory index; smem offset in tile order
+                    idx = np.indices(box[::-1]).reshape(5, -1)[::-1]       # i0 fastest
+                    addr = (c[0] + idx[0]) * 8
+                    for d in range(1, 5):
+                        addr = addr + (c[d] + idx[d]) * strides[d - 1]
+                    mem = addr // 8
+                    smem_l = cpy * (box_bytes // 8) + np.arange(idx.shape[1])
+                    want = np.array([base | mem_of(int(l)) for l in smem_l])
+                    assert np.array_equal(mem, want)
