@@ -263,46 +263,49 @@ k_tc_chain(const __grid_constant__ CUtensorMap tmap, const ChainGeom geom, TileW
                 }
             }
         }
-    } else if (tid == kLoadWarp) {
-        // ---- HBM traffic: one thread, TMA tensor copies --------------------
-        // Tile k goes into buffer k % 3 once tile k - 3's staged result has
-        // been stored from it (its shared-memory reads done).
-        const CUtensorMap* map = &tmap;
-        const uint64_t mine = blockIdx.x < ntiles ? (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
-        const uint32_t copies = 1u << geom.n_rem;
-        bool ok = true;
-        auto store = [&](uint64_t k) -> bool {
-            const uint32_t b = static_cast<uint32_t>(k % kBufs);
-            if (!mbar_wait_bounded(&staged[b], static_cast<uint32_t>(k / kBufs) & 1u)) return false;
-            const uint64_t tile = blockIdx.x + k * gridDim.x;
-            const uint32_t src = smem_u32(bufs + b * kBufBytes);
-            for (uint32_t cpy = 0; cpy < copies; ++cpy) {
-                int c[5];
-                tile_coords(P, geom, tile, cpy, c);
-                tma_store_5d(map, c, src + cpy * geom.box_bytes);
+    } else if (tid >= kLoadWarp) {
+        // ---- HBM traffic: one thread of the load warp, TMA tensor copies -----
+        // (the warp's other lanes only wait at the end).  Tile k goes into
+        // buffer k % 3 once tile k - 3's staged result has been stored from it
+        // (its shared-memory reads done).
+        if (tid == kLoadWarp) {
+            const CUtensorMap* map = &tmap;
+            const uint64_t mine = blockIdx.x < ntiles ? (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+            const uint32_t copies = 1u << geom.n_rem;
+            bool ok = true;
+            auto store = [&](uint64_t k) -> bool {
+                const uint32_t b = static_cast<uint32_t>(k % kBufs);
+                if (!mbar_wait_bounded(&staged[b], static_cast<uint32_t>(k / kBufs) & 1u)) return false;
+                const uint64_t tile = blockIdx.x + k * gridDim.x;
+                const uint32_t src = smem_u32(bufs + b * kBufBytes);
+                for (uint32_t cpy = 0; cpy < copies; ++cpy) {
+                    int c[5];
+                    tile_coords(P, geom, tile, cpy, c);
+                    tma_store_5d(map, c, src + cpy * geom.box_bytes);
+                }
+                bulk_commit();
+                return true;
+            };
+            for (uint64_t k = 0; k < mine && ok; ++k) {
+                const uint32_t b = static_cast<uint32_t>(k % kBufs);
+                if (k >= kBufs) {
+                    ok = store(k - kBufs);
+                    bulk_wait_read();        // the buffer has been read out
+                    if (!ok) break;
+                }
+                const uint64_t tile = blockIdx.x + k * gridDim.x;
+                const uint32_t dst = smem_u32(bufs + b * kBufBytes);
+                mbar_arrive_expect_tx(&full[b], kBufBytes);
+                for (uint32_t cpy = 0; cpy < copies; ++cpy) {
+                    int c[5];
+                    tile_coords(P, geom, tile, cpy, c);
+                    tma_load_5d(dst + cpy * geom.box_bytes, map, c, &full[b]);
+                }
             }
-            bulk_commit();
-            return true;
-        };
-        for (uint64_t k = 0; k < mine && ok; ++k) {
-            const uint32_t b = static_cast<uint32_t>(k % kBufs);
-            if (k >= kBufs) {
-                ok = store(k - kBufs);
-                bulk_wait_read();        // the buffer has been read out
-                if (!ok) break;
-            }
-            const uint64_t tile = blockIdx.x + k * gridDim.x;
-            const uint32_t dst = smem_u32(bufs + b * kBufBytes);
-            mbar_arrive_expect_tx(&full[b], kBufBytes);
-            for (uint32_t cpy = 0; cpy < copies; ++cpy) {
-                int c[5];
-                tile_coords(P, geom, tile, cpy, c);
-                tma_load_5d(dst + cpy * geom.box_bytes, map, c, &full[b]);
-            }
+            for (uint64_t k = mine > kBufs ? mine - kBufs : 0; k < mine && ok; ++k) ok = store(k);
+            bulk_wait_all();
+            if (!ok) atomicExch(err, 4);
         }
-        for (uint64_t k = mine > kBufs ? mine - kBufs : 0; k < mine && ok; ++k) ok = store(k);
-        bulk_wait_all();
-        if (!ok) atomicExch(err, 4);
     } else {
         // ---- the compute warps: two slots, one step each per round -----------
         const uint32_t t = tid;
@@ -464,6 +467,9 @@ k_tc_chain(const __grid_constant__ CUtensorMap tmap, const ChainGeom geom, TileW
         for (uint32_t s = 0; s < 2; ++s)
             if (pending[s]) mbar_wait_bounded(&mmab[s], uses[s] & 1u);
     }
+    // The load and MMA warps ran one thread's code: reconverge each warp
+    // before the block-wide barrier, whose aligned form needs whole warps.
+    __syncwarp();
     tc_fence_before();
     __syncthreads();
     if (tid < 32) {
