@@ -14,24 +14,19 @@
 // tensor-memory columns and its own B staging): while slot 0's MMAs run,
 // the 256 compute threads convert slot 1's tile, and the other way round.
 // Slot 1 starts half a tile behind slot 0, so its buffer's next load has
-// time to land.  One thread of a ninth warp moves every tile between HBM and
-// three 64 KB buffers with TMA tensor copies: the state is viewed as a
-// 5-dimensional tensor whose dimensions start at the tile's runs of
-// consecutive memory qubits, so a tile is one box (or a few, when it has
-// more than five runs) and a copy's coordinates are the tile's other
-// qubits.  The last op's result is staged in its buffer in tile order and
-// stored by the same thread, which then reloads the buffer.  A tenth warp
-// issues the MMAs: a slot's 256 threads arrive on its "A ready" barrier
-// after writing A and B and go on to the other slot at once, so an MMA
-// issue that waits for the tensor pipe to drain the other slot's MMAs
+// time to land.  Three producer warps move the tiles between HBM and three
+// 64 KB buffers: 16-byte cp.async pieces (TMA bulk copies for runs of
+// >= 4 KB) into a buffer, and, after the last op, the result that the
+// compute warps staged in the buffer in tile order back to HBM with
+// 16-byte stores; then the buffer takes the tile three ahead.  A twelfth
+// warp issues the MMAs: a slot's 256 threads arrive on its "A ready"
+// barrier after writing A and B and go on to the other slot at once, so an
+// MMA issue that waits for the tensor pipe to drain the other slot's MMAs
 // stalls nobody.  HBM traffic: 16 B per amplitude per pass.
 //
 // Every wait is bounded (2 s / 2^26 polls); on expiry the CTA raises *err,
 // waits (bounded) for its own MMAs and copies, frees its tensor memory and
 // returns.
-#include <cuda.h>
-#include <cudaTypedefs.h>
-
 #include "common.cuh"
 #include "tc_ptx.cuh"
 #include "tile.h"
@@ -43,14 +38,16 @@ namespace {
 using namespace ptx;
 
 constexpr int kCompute = 256;                     // thread t converts A / D row t
-constexpr int kLoadWarp = kCompute;               // first thread of the load warp
-constexpr int kMmaWarp = kCompute + 32;           // first thread of the MMA warp
-constexpr int kThreads = kCompute + 64;
+constexpr int kProducers = 96;                    // warps 8..10: HBM <-> buffers
+constexpr int kMmaThread = kCompute + kProducers; // warp 11, first lane: MMA issue
+constexpr int kThreads = kCompute + kProducers + 32;
 constexpr uint32_t kTile = 1u << kTileQubits;
 constexpr uint32_t kBufBytes = kTile * 8u;        // 64 KB: the tile (fp32) or its A operand (bf16 hi | lo)
 constexpr uint32_t kBufs = 3;
+constexpr uint32_t kBulkMin = 9;                  // runs of >= 2^9 amplitudes load by bulk copies
 constexpr size_t kOffB = size_t{kBufs} * kBufBytes;
-constexpr size_t kOffPass = kOffB + 2 * kTcBBytes;
+constexpr size_t kOffRow = kOffB + 2 * kTcBBytes;                   // u64[128]: memory offset of piece row c
+constexpr size_t kOffPass = kOffRow + 128 * 8;
 constexpr size_t kOffPhases = kOffPass + sizeof(TilePass);
 constexpr size_t kOffBoff = kOffPhases + kMaxSmemPhases * sizeof(TilePhase);
 constexpr size_t kOffBar = (kOffBoff + kMaxSmemPhases * 4 + 7) & ~size_t{7};
@@ -62,52 +59,26 @@ static_assert(kSmemChain <= 227 * 1024, "shared memory per CTA");
 constexpr uint32_t kBPerThread = kTcBBytes / (16u * kCompute);   // 4 x 16 B of B per thread
 constexpr uint32_t kTmemCols = 512;               // two slots x (2 M-blocks x (D1 | D2))
 
-// The tile as TMA boxes: the state is a 5-D tensor of 8-byte amplitudes
-// whose dimension d covers memory qubits [lo[d], lo[d+1]) (the last real
-// one up to n); a tile's runs of consecutive memory qubits (at most 8 per
-// dimension) sit at the bottom of the first five dimensions, so a box holds
-// them in tile order.  Tile qubits beyond the fifth run (rem_q, ascending)
-// are enumerated by 2^n_rem copies of box_bytes each, in tile order too.
-// A tile's coordinates are its out qubits, each at bit (q - lo[d]) of the
-// dimension d that contains it.
-struct ChainGeom {
-    uint8_t lo[5];       // first memory qubit of each dimension (64: unused dimension)
-    uint8_t n_rem;
-    uint8_t rem_q[13];
-    uint8_t pad[3];
-    uint32_t box_bytes;
-};
+__device__ __forceinline__ uint64_t tile_base(const TilePass& P, uint64_t tile) {
+    uint64_t base = 0;
+    for (uint32_t j = 0; j < P.n_out; ++j, tile >>= 1)
+        if (tile & 1u) base |= uint64_t{1} << P.out_mem[j];
+    return base;
+}
 
-__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map, const int (&c)[5], uint64_t* bar) {
+// Barrier 2 over the 96 producer threads.
+__device__ __forceinline__ void producer_sync() { asm volatile("bar.sync 2, 96;" ::: "memory"); }
+__device__ __forceinline__ bool producer_any(bool x) {
+    uint32_t r;
     asm volatile(
-        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
-        "%6}], [%7];" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(smem_u32(bar))
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, 2, 96, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"(x ? 1u : 0u)
         : "memory");
-}
-__device__ __forceinline__ void tma_store_5d(const CUtensorMap* map, const int (&c)[5], uint32_t src) {
-    asm volatile("cp.async.bulk.tensor.5d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4, %5}], [%6];" ::"l"(
-                     reinterpret_cast<uint64_t>(map)),
-                 "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(src)
-                 : "memory");
-}
-
-// Coordinates of copy `cpy` of tile `tile`.
-__device__ __forceinline__ void tile_coords(const TilePass& P, const ChainGeom& g, uint64_t tile, uint32_t cpy,
-                                            int (&c)[5]) {
-#pragma unroll
-    for (int d = 0; d < 5; ++d) c[d] = 0;
-    for (uint32_t j = 0; j < P.n_out; ++j, tile >>= 1) {
-        if (!(tile & 1u)) continue;
-        const uint32_t q = P.out_mem[j];
-        int d = 0;
-#pragma unroll
-        for (int k = 1; k < 5; ++k)
-            if (g.lo[k] <= q) d = k;
-        c[d] |= 1 << (q - g.lo[d]);
-    }
-    for (uint32_t i = 0; i < g.n_rem; ++i)
-        if ((cpy >> i) & 1u) c[4] |= 1 << (g.rem_q[i] - g.lo[4]);
+    return r != 0;
 }
 
 // Barrier 1 over the 256 compute threads (the load warp never joins it).
@@ -176,11 +147,11 @@ __device__ __forceinline__ void scatter16(const float2 (&v)[16], uint32_t base_r
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
-k_tc_chain(const __grid_constant__ CUtensorMap tmap, const ChainGeom geom, TileWork w, uint64_t ntiles,
-           int* __restrict__ err) {
+k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char* bufs = smem;
     unsigned char* bstage = smem + kOffB;
+    uint64_t* rowoff = reinterpret_cast<uint64_t*>(smem + kOffRow);
     TilePass* sp = reinterpret_cast<TilePass*>(smem + kOffPass);
     TilePhase* sph = reinterpret_cast<TilePhase*>(smem + kOffPhases);
     uint32_t* sboff = reinterpret_cast<uint32_t*>(smem + kOffBoff);
@@ -204,15 +175,24 @@ k_tc_chain(const __grid_constant__ CUtensorMap tmap, const ChainGeom geom, TileW
             const TilePhase& ph = w.phases[pb + tid];
             sboff[tid] = ph.op_end > ph.op_begin ? w.ops[ph.op_begin].data : 0u;
         }
+        // piece rows: 16-byte piece i = l + 32 c of a tile holds tile-local
+        // amplitudes 2 i, 2 i + 1 (bits 1..5 from l, 6..12 from c); rowoff[c]
+        // is the memory offset of c's bits
+        if (tid < 128) {
+            uint64_t o = 0;
+            for (int i = 0; i < 7; ++i)
+                if ((tid >> i) & 1u) o |= uint64_t{1} << GP.tile_pos[6 + i];
+            rowoff[tid] = o;
+        }
     }
     if (tid == 0) {
         for (int b = 0; b < 3; ++b) {
-            mbar_init(&full[b], 1);          // the loading thread's expect_tx arrival
-            mbar_init(&staged[b], kCompute); // every compute thread, after its writes
+            mbar_init(&full[b], kProducers);    // one (deferred) arrival per producer thread
+            mbar_init(&staged[b], kCompute);    // every compute thread, after its writes
         }
         mbar_init(&mmab[0], 1);
         mbar_init(&mmab[1], 1);
-        mbar_init(&aready[0], kCompute);    // every compute thread, after its writes
+        mbar_init(&aready[0], kCompute);
         mbar_init(&aready[1], kCompute);
         fence_mbar_init();
     }
@@ -231,15 +211,15 @@ k_tc_chain(const __grid_constant__ CUtensorMap tmap, const ChainGeom geom, TileW
     const uint32_t first = sph[0].op_end > sph[0].op_begin ? 0u : 1u;
     const uint32_t last = sph[nph - 1].op_end > sph[nph - 1].op_begin ? nph - 1 : nph - 2;
     const uint32_t m = last - first + 1;           // tensor-core ops per tile
+    const uint64_t mine = blockIdx.x < ntiles ? (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
 
-    if (tid >= kMmaWarp) {
-        // ---- the MMA warp: one thread issues each slot's MMAs once its A and
-        // B are written (slots in whatever order they become ready) ----------
-        if (tid == kMmaWarp) {
-            const uint64_t mine = blockIdx.x < ntiles ? (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    if (tid >= kMmaThread) {
+        // ---- the MMA warp: its first thread issues each slot's MMAs once the
+        // slot's A and B are written, slots in whichever order they get ready
+        if (tid == kMmaThread) {
             uint64_t left[2] = {m * ((mine + 1) / 2), m * (mine / 2)};
             uint32_t ph[2] = {0u, 0u};
-            uint64_t last = global_ns();
+            uint64_t last_ns = global_ns();
             uint32_t spins = 0;
             while (left[0] + left[1] > 0) {
                 bool did = false;
@@ -253,59 +233,76 @@ k_tc_chain(const __grid_constant__ CUtensorMap tmap, const ChainGeom geom, TileW
                     }
                 }
                 if (did) {
-                    last = global_ns();
+                    last_ns = global_ns();
                 } else if (++spins >= 1024u) {
                     spins = 0;
-                    if (global_ns() - last > 2000000000ull) {   // the compute warps stopped: give up
+                    if (global_ns() - last_ns > 2000000000ull) {   // the compute warps stopped: give up
                         atomicExch(err, 5);
                         break;
                     }
                 }
             }
         }
-    } else if (tid >= kLoadWarp) {
-        // ---- HBM traffic: one thread of the load warp, TMA tensor copies -----
-        // (the warp's other lanes only wait at the end).  Tile k goes into
-        // buffer k % 3 once tile k - 3's staged result has been stored from it
-        // (its shared-memory reads done).
-        if (tid == kLoadWarp) {
-            const CUtensorMap* map = &tmap;
-            const uint64_t mine = blockIdx.x < ntiles ? (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
-            const uint32_t copies = 1u << geom.n_rem;
-            bool ok = true;
-            auto store = [&](uint64_t k) -> bool {
-                const uint32_t b = static_cast<uint32_t>(k % kBufs);
-                if (!mbar_wait_bounded(&staged[b], static_cast<uint32_t>(k / kBufs) & 1u)) return false;
-                const uint64_t tile = blockIdx.x + k * gridDim.x;
-                const uint32_t src = smem_u32(bufs + b * kBufBytes);
-                for (uint32_t cpy = 0; cpy < copies; ++cpy) {
-                    int c[5];
-                    tile_coords(P, geom, tile, cpy, c);
-                    tma_store_5d(map, c, src + cpy * geom.box_bytes);
-                }
-                bulk_commit();
-                return true;
-            };
-            for (uint64_t k = 0; k < mine && ok; ++k) {
-                const uint32_t b = static_cast<uint32_t>(k % kBufs);
-                if (k >= kBufs) {
-                    ok = store(k - kBufs);
-                    bulk_wait_read();        // the buffer has been read out
-                    if (!ok) break;
-                }
-                const uint64_t tile = blockIdx.x + k * gridDim.x;
-                const uint32_t dst = smem_u32(bufs + b * kBufBytes);
-                mbar_arrive_expect_tx(&full[b], kBufBytes);
-                for (uint32_t cpy = 0; cpy < copies; ++cpy) {
-                    int c[5];
-                    tile_coords(P, geom, tile, cpy, c);
-                    tma_load_5d(dst + cpy * geom.box_bytes, map, c, &full[b]);
-                }
+    } else if (tid >= kCompute) {
+        // ---- the producer warps: tile k goes into buffer k % 3 after tile
+        // k - 3's staged result has been stored from it ------------------------
+        const uint32_t pt = tid - kCompute;            // 0..95
+        const uint32_t lane = pt & 31u, pw = pt >> 5;  // pw: 0..2 takes piece rows c = pw, pw + 3, ...
+        const uint32_t nl = P.n_low;
+        float2* __restrict__ state = w.state;
+        uint64_t gl = 0;
+#pragma unroll
+        for (int i = 0; i < 5; ++i)
+            if ((lane >> i) & 1u) gl |= uint64_t{1} << P.tile_pos[1 + i];
+        bool ok = true;
+        auto store = [&](uint64_t k) -> bool {
+            const uint32_t b = static_cast<uint32_t>(k % kBufs);
+            const bool got = mbar_wait_bounded(&staged[b], static_cast<uint32_t>(k / kBufs) & 1u);
+            if (producer_any(!got)) return false;
+            const uint64_t g0 = tile_base(P, blockIdx.x + k * gridDim.x) | gl;
+            const uint4* src = reinterpret_cast<const uint4*>(bufs + b * kBufBytes) + lane;
+            uint4* dst = reinterpret_cast<uint4*>(state);
+            for (uint32_t c = pw; c < 128; c += 3) {
+                const uint4 v = src[32 * c];
+                dst[(g0 | rowoff[c]) >> 1] = v;     // amplitudes g, g + 1 (g even)
             }
-            for (uint64_t k = mine > kBufs ? mine - kBufs : 0; k < mine && ok; ++k) ok = store(k);
-            bulk_wait_all();
-            if (!ok) atomicExch(err, 4);
+            return true;
+        };
+        for (uint64_t k = 0; k < mine && ok; ++k) {
+            const uint32_t b = static_cast<uint32_t>(k % kBufs);
+            unsigned char* buf = bufs + b * kBufBytes;
+            if (k >= kBufs) {
+                ok = store(k - kBufs);
+                producer_sync();          // every producer has read the buffer out
+                if (!ok) break;
+            }
+            fence_proxy_async();          // generic reads of the buffer precede the copies into it
+            const uint64_t base = tile_base(P, blockIdx.x + k * gridDim.x);
+            if (nl >= kBulkMin) {
+                const uint32_t chunks = 1u << (kTileQubits - nl);
+                const uint32_t bytes = (1u << nl) * 8u;
+                if (pt == 0) mbar_arrive_expect_tx(&full[b], kBufBytes);
+                for (uint32_t c = pt; c < chunks; c += kProducers) {
+                    uint64_t g = base;
+                    for (uint32_t j = nl; j < static_cast<uint32_t>(kTileQubits); ++j)
+                        if ((c >> (j - nl)) & 1u) g |= uint64_t{1} << P.tile_pos[j];
+                    bulk_g2s(buf + (static_cast<size_t>(c) << nl) * 8u, state + g, bytes, &full[b]);
+                }
+                if (pt != 0) mbar_arrive(&full[b]);
+            } else {
+                const uint32_t d0 = smem_u32(buf) + 16u * lane;
+                const uint64_t g0 = base | gl;
+                for (uint32_t c = pw; c < 128; c += 3)
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d0 + 512u * c),
+                                 "l"(state + (g0 | rowoff[c]))
+                                 : "memory");
+                asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(&full[b]))
+                             : "memory");
+            }
         }
+        for (uint64_t k = mine > kBufs ? mine - kBufs : 0; k < mine && ok; ++k) ok = store(k);
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        if (!ok && pt == 0) atomicExch(err, 4);
     } else {
         // ---- the compute warps: two slots, one step each per round -----------
         const uint32_t t = tid;
@@ -480,61 +477,9 @@ k_tc_chain(const __grid_constant__ CUtensorMap tmap, const ChainGeom geom, TileW
 
 }  // namespace
 
-// The tile's TMA geometry and tensor map over `state` (see ChainGeom).
-static bool chain_tensor_map(const TilePass& P, uint32_t n, float2* state, CUtensorMap* map, ChainGeom* g) {
-    // runs of consecutive memory qubits, at most 8 long (a box side is <= 256)
-    uint32_t run_lo[kTileQubits], run_len[kTileQubits], nr = 0;
-    for (int i = 0; i < kTileQubits;) {
-        uint32_t len = 1;
-        while (i + static_cast<int>(len) < kTileQubits && len < 8 && P.tile_pos[i + len] == P.tile_pos[i] + len) ++len;
-        run_lo[nr] = P.tile_pos[i];
-        run_len[nr++] = len;
-        i += static_cast<int>(len);
-    }
-    const uint32_t nd = nr < 5 ? nr : 5;     // real dimensions
-    cuuint64_t dims[5], strides[4];
-    cuuint32_t box[5], estr[5] = {1, 1, 1, 1, 1};
-    *g = ChainGeom{};
-    uint32_t boxed = 0;
-    for (uint32_t d = 0; d < 5; ++d) {
-        if (d < nd) {
-            g->lo[d] = static_cast<uint8_t>(run_lo[d]);
-            const uint32_t hi = (d + 1 < nd) ? run_lo[d + 1] : n;
-            dims[d] = cuuint64_t{1} << (hi - run_lo[d]);
-            box[d] = 1u << run_len[d];
-            boxed += run_len[d];
-        } else {
-            g->lo[d] = 64;
-            dims[d] = 1;
-            box[d] = 1;
-        }
-        if (d > 0) strides[d - 1] = d < nd ? cuuint64_t{8} << run_lo[d] : cuuint64_t{8} << n;
-    }
-    g->n_rem = 0;
-    for (uint32_t r = nd; r < nr; ++r)
-        for (uint32_t k = 0; k < run_len[r]; ++k) g->rem_q[g->n_rem++] = static_cast<uint8_t>(run_lo[r] + k);
-    g->box_bytes = 8u << boxed;
-    if (boxed + g->n_rem != static_cast<uint32_t>(kTileQubits) || run_lo[0] != 0) return false;
-    // the driver's encoder, looked up through the runtime (no link-time
-    // dependency on the driver library, which hosts without a GPU lack)
-    static PFN_cuTensorMapEncodeTiled encode = nullptr;
-    if (!encode) {
-        void* fn = nullptr;
-        cudaDriverEntryPointQueryResult q{};
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess || !fn)
-            return false;
-        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(fn);
-    }
-    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 5, state, dims, strides, box, estr,
-                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    return r == CUDA_SUCCESS;
-}
-
-cudaError_t launch_chain_pass(float2* state, uint32_t n, const TilePass& host_pass, const TilePass* d_passes,
-                              const TilePhase* d_phases, const TileOp* d_ops, const float2* d_mats,
-                              uint32_t pass_index, int* err, cudaStream_t s) {
+cudaError_t launch_chain_pass(float2* state, uint32_t n, const TilePass* d_passes, const TilePhase* d_phases,
+                              const TileOp* d_ops, const float2* d_mats, uint32_t pass_index, int* err,
+                              cudaStream_t s) {
     static bool configured = false;
     if (!configured) {
         const cudaError_t e = cudaFuncSetAttribute(k_tc_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -542,14 +487,11 @@ cudaError_t launch_chain_pass(float2* state, uint32_t n, const TilePass& host_pa
         if (e != cudaSuccess) return e;
         configured = true;
     }
-    CUtensorMap map;
-    ChainGeom geom;
-    if (!chain_tensor_map(host_pass, n, state, &map, &geom)) return cudaErrorInvalidValue;
     const uint64_t tiles = uint64_t{1} << (n - kTileQubits);
     uint64_t grid = static_cast<uint64_t>(sm_count());
     if (grid > tiles) grid = tiles;
     const TileWork w{state, 0, d_passes, d_phases, d_ops, d_mats, pass_index, 0};
-    k_tc_chain<<<static_cast<unsigned>(grid), kThreads, kSmemChain, s>>>(map, geom, w, tiles, err);
+    k_tc_chain<<<static_cast<unsigned>(grid), kThreads, kSmemChain, s>>>(w, tiles, err);
     return cudaGetLastError();
 }
 

@@ -32,7 +32,6 @@ struct qlb_plan {
     uint32_t n = 0;
     int mode = 0;
     std::vector<qlb::PlanStep> steps;
-    std::vector<qlb::TilePass> host_passes;   // host copies (the chain kernel's tensor maps)
     qlb::DeviceBuffer dev;   // [passes | phases | ops | matrices]
     const void* image = nullptr;   // the device image: dev.p, or a buffer the engine lends for one execute()
     size_t o_pass = 0, o_phase = 0, o_ops = 0, o_mat = 0;

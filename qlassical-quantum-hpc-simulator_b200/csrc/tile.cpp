@@ -1417,7 +1417,6 @@ qlb_plan* compile_plan(qlb_engine& e, const qlb_gate_instr* prog, uint64_t count
         p->n = e.sv.n;
         p->mode = e.mode;
         p->steps = std::move(pl.steps);
-        p->host_passes = tp.passes;
         p->stats = pl.stats;
         p->stats.instructions = count;
         p->stats.sweep_bytes = static_cast<double>(p->stats.sweeps) * 16.0 * static_cast<double>(uint64_t{1} << e.sv.n);
@@ -1598,8 +1597,7 @@ void run_plan(qlb_engine& e, const qlb_plan& p) {
         switch (st.kind) {
         case STEP_PASS:
             if (st.features & kPassChain) {
-                check_cuda(launch_chain_pass(e.sv.d, e.sv.n, p.host_passes[st.index],
-                                             reinterpret_cast<const TilePass*>(d + p.o_pass),
+                check_cuda(launch_chain_pass(e.sv.d, e.sv.n, reinterpret_cast<const TilePass*>(d + p.o_pass),
                                              reinterpret_cast<const TilePhase*>(d + p.o_phase),
                                              reinterpret_cast<const TileOp*>(d + p.o_ops), mats, st.index,
                                              static_cast<int*>(e.err_flag.p), e.stream),

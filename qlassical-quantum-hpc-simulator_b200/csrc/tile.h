@@ -210,11 +210,10 @@ cudaError_t launch_tile_pass(float2* state, uint32_t n, const TilePass* d_passes
 int sm_count();   // multiprocessors of the current device (cached)
 
 // The chain kernel (chain.cu): one launch applies chain pass `pass_index`
-// to the state; `host_pass` is the host copy of that pass (its tile qubits
-// define the TMA tensor map); returns the launch status.
-cudaError_t launch_chain_pass(float2* state, uint32_t n, const TilePass& host_pass, const TilePass* d_passes,
-                              const TilePhase* d_phases, const TileOp* d_ops, const float2* d_mats,
-                              uint32_t pass_index, int* err, cudaStream_t s);
+// to the state; returns the launch status.
+cudaError_t launch_chain_pass(float2* state, uint32_t n, const TilePass* d_passes, const TilePhase* d_phases,
+                              const TileOp* d_ops, const float2* d_mats, uint32_t pass_index, int* err,
+                              cudaStream_t s);
 
 // Runs the tile kernel's bounded mbarrier wait on a barrier that never
 // completes; *err becomes 1 when the wait gives up (as it must).

@@ -131,102 +131,24 @@ def test_chain_passes_of_the_fused_rotation_circuit(n, depth):
     assert oracle.infidelity(want, got) < 1e-6
 
 
-def test_chain_load_warp_addressing():
-    """The chain kernel's load warp walks its 128 16-byte pieces per lane in
-    Gray-code order, XOR-ing one memory bit and one buffer-offset bit per
-    step (chain.cu).  Replayed here: every piece of the 64 KB buffer is
-    written exactly once, at an offset inside the buffer, from the memory
-    index its tile-local index maps to."""
+def test_chain_producer_piece_addressing():
+    """The chain kernel's producer warps move 16-byte pieces: piece i =
+    lane + 32 c of a tile holds tile-local amplitudes 2 i, 2 i + 1, at
+    memory index (lane's bits 1..5 -> tile qubits 1..5) | rowoff[c] (c's
+    bits -> tile qubits 6..12) (chain.cu).  Every piece of the 64 KB buffer
+    is covered exactly once, from the memory index its tile-local index
+    maps to; producer warp w takes the rows c = w, w + 3, ..."""
     rng = np.random.default_rng(3)
     for _ in range(4):
         tp = [0, 1, 2] + sorted(int(x) for x in rng.choice(np.arange(3, 30), 10, replace=False))
         mem_of = lambda l: sum(1 << tp[j] for j in range(13) if (l >> j) & 1)   # noqa: E731
-        hb = [1 << tp[6 + i] for i in range(7)]
+        rowoff = [sum(1 << tp[6 + i] for i in range(7) if (c >> i) & 1) for c in range(128)]
         seen = {}
-        for lane in range(32):
-            gl = sum(1 << tp[1 + i] for i in range(5) if (lane >> i) & 1)
-            g, d = gl, 16 * lane
-            for hi in range(16):
-                if hi:
-                    bit = (hi & -hi).bit_length() - 1
-                    g ^= hb[3 + bit]
-                    d ^= 4096 << bit
-                for lo in range(8):
-                    if lo:
-                        bit = 0 if lo & 1 else (1 if lo & 2 else 2)
-                        g ^= hb[bit]
-                        d ^= 512 << bit
-                    assert 0 <= d < 65536 and d % 16 == 0 and d not in seen
-                    seen[d] = g
-                g ^= hb[2]
-                d ^= 2048
-        assert len(seen) == 4096
-        for d, g in seen.items():
-            assert g == mem_of(d // 8)
-
-
-def _chain_geometry(tp, n):
-    """chain.cu's chain_tensor_map(): dimensions at the tile's runs of
-    consecutive memory qubits (at most 8 long), the first five boxed, the
-    rest enumerated by copies."""
-    runs, i = [], 0
-    while i < 13:
-        ln = 1
-        while i + ln < 13 and ln < 8 and tp[i + ln] == tp[i] + ln:
-            ln += 1
-        runs.append((tp[i], ln))
-        i += ln
-    nd = min(len(runs), 5)
-    lo = [runs[d][0] if d < nd else 64 for d in range(5)]
-    dims, box, strides = [], [], []
-    for d in range(5):
-        if d < nd:
-            hi = runs[d + 1][0] if d + 1 < nd else n
-            dims.append(1 << (hi - runs[d][0]))
-            box.append(1 << runs[d][1])
-        else:
-            dims.append(1)
-            box.append(1)
-        if d > 0:
-            strides.append(8 << runs[d][0] if d < nd else 8 << n)
-    rem = [runs[r][0] + k for r in range(nd, len(runs)) for k in range(runs[r][1])]
-    boxed = sum(runs[d][1] for d in range(nd))
-    return lo, dims, box, strides, rem, 8 << boxed
-
-
-def test_chain_tma_geometry():
-    """Every TMA box of every tile lands its amplitudes at their tile-order
-    offsets, inside the tensor and the 64 KB buffer, with 16-byte-aligned
-    starts (chain.cu: chain_tensor_map, tile_coords)."""
-    rng = np.random.default_rng(11)
-    for n in (14, 17, 20, 30, 34):
-        for _ in range(6):
-            others = sorted(int(x) for x in rng.choice(np.arange(3, n), 10, replace=False))
-            tp = [0, 1, 2] + others
-            lo, dims, box, strides, rem, box_bytes = _chain_geometry(tp, n)
-            out = [q for q in range(n) if q not in tp]
-            assert box_bytes * (1 << len(rem)) == 65536 and box[0] * 8 % 16 == 0
-            assert all(st % 16 == 0 and st < 2 ** 40 for st in strides)
-            assert all(b <= 256 and b <= dm for b, dm in zip(box, dims)) and all(dm < 2 ** 32 for dm in dims)
-            mem_of = lambda l: sum(1 << tp[j] for j in range(13) if (l >> j) & 1)   # noqa: E731
-            for tile in [0, 1, (1 << (n - 13)) - 1, int(rng.integers(0, 1 << (n - 13)))]:
-                base = sum(1 << out[j] for j in range(len(out)) if (tile >> j) & 1)
-                for cpy in range(1 << len(rem)):
-                    c = [0] * 5
-                    for j, q in enumerate(out):
-                        if (tile >> j) & 1:
-                            d = max(k for k in range(5) if lo[k] <= q)
-                            c[d] |= 1 << (q - lo[d])
-                    for i, q in enumerate(rem):
-                        if (cpy >> i) & 1:
-                            c[4] |= 1 << (q - lo[4])
-                    assert all(c[d] + box[d] <= dims[d] for d in range(5)) and (c[0] * 8) % 16 == 0
-                    # box element (i0..i4) -> tensor element -> memory index; smem offset in tile order
-                    idx = np.indices(box[::-1]).reshape(5, -1)[::-1]       # i0 fastest
-                    addr = (c[0] + idx[0]) * 8
-                    for d in range(1, 5):
-                        addr = addr + (c[d] + idx[d]) * strides[d - 1]
-                    mem = addr // 8
-                    smem_l = cpy * (box_bytes // 8) + np.arange(idx.shape[1])
-                    want = np.array([base | mem_of(int(l)) for l in smem_l])
-                    assert np.array_equal(mem, want)
+        for pw in range(3):
+            for lane in range(32):
+                gl = sum(1 << tp[1 + i] for i in range(5) if (lane >> i) & 1)
+                for c in range(pw, 128, 3):
+                    d = 16 * lane + 512 * c
+                    assert d not in seen
+                    seen[d] = gl | rowoff[c]
+        assert len(seen) == 4096 and all(g == mem_of(d // 8) for d, g in seen.items())
