@@ -17,8 +17,8 @@
 // time to land.  Three producer warps move the tiles between HBM and three
 // 64 KB buffers: 16-byte cp.async pieces (TMA bulk copies for runs of
 // >= 4 KB) into a buffer, and, after the last op, the result that the
-// compute warps staged in the buffer in tile order back to HBM with
-// 16-byte stores; then the buffer takes the tile three ahead.  A twelfth
+// compute warps staged in the buffer (bank-swizzled tile order) back to
+// HBM with 16-byte stores; then the buffer takes the tile three ahead.  A twelfth
 // warp issues the MMAs: a slot's 256 threads arrive on its "A ready"
 // barrier after writing A and B and go on to the other slot at once, so an
 // MMA issue that waits for the tensor pipe to drain the other slot's MMAs
@@ -65,6 +65,8 @@ __device__ __forceinline__ uint64_t tile_base(const TilePass& P, uint64_t tile) 
         if (tile & 1u) base |= uint64_t{1} << P.out_mem[j];
     return base;
 }
+
+__device__ __forceinline__ uint32_t fold4(uint32_t i) { return ((i >> 4) ^ (i >> 8) ^ (i >> 12)) & 15u; }
 
 // Barrier 2 over the 96 producer threads.
 __device__ __forceinline__ void producer_sync() { asm volatile("bar.sync 2, 96;" ::: "memory"); }
@@ -259,11 +261,17 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
             const uint32_t b = static_cast<uint32_t>(k % kBufs);
             const bool got = mbar_wait_bounded(&staged[b], static_cast<uint32_t>(k / kBufs) & 1u);
             if (producer_any(!got)) return false;
+            // piece i = lane + 32 c (amplitudes 2 i, 2 i + 1) sits in 16-byte
+            // unit i ^ (F >> 1) of the staged layout, halves swapped when F is
+            // odd, F = fold4(2 i) = fold4(2 lane) ^ fold4(64 c)
             const uint64_t g0 = tile_base(P, blockIdx.x + k * gridDim.x) | gl;
-            const uint4* src = reinterpret_cast<const uint4*>(bufs + b * kBufBytes) + lane;
+            const uint4* src = reinterpret_cast<const uint4*>(bufs + b * kBufBytes);
             uint4* dst = reinterpret_cast<uint4*>(state);
+            const uint32_t fl = fold4(2u * lane);
             for (uint32_t c = pw; c < 128; c += 3) {
-                const uint4 v = src[32 * c];
+                const uint32_t f = fl ^ fold4(64u * c);
+                uint4 v = src[(lane + 32u * c) ^ (f >> 1)];
+                if (f & 1u) v = make_uint4(v.z, v.w, v.x, v.y);
                 dst[(g0 | rowoff[c]) >> 1] = v;     // amplitudes g, g + 1 (g even)
             }
             return true;
@@ -394,15 +402,21 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                     }
                     tc_fence_after();
                     if (j == m) {
-                        // the last op's result, staged in its (now free) buffer
-                        // in tile order for the TMA store
+                        // the last op's result, staged in its (now free) buffer:
+                        // amplitude l at 8-byte word l ^ fold4(l) (the fold spreads
+                        // a warp's stores over the banks; it leaves bit 0 alone, so
+                        // amplitudes 2i, 2i + 1 share a 16-byte unit)
                         const TilePhase& L = sph[last];
                         uint32_t lt = 0, le[kRegQubits];
 #pragma unroll
                         for (int i = 0; i < kThreadQubits; ++i)
                             if ((t >> i) & 1u) lt |= 1u << L.thr_pos[i];
+                        lt ^= fold4(lt);
 #pragma unroll
-                        for (int i = 0; i < kRegQubits; ++i) le[i] = 1u << L.reg_pos[i];
+                        for (int i = 0; i < kRegQubits; ++i) {
+                            le[i] = 1u << L.reg_pos[i];
+                            le[i] ^= fold4(le[i]);
+                        }
                         float2* dst = reinterpret_cast<float2*>(buf);
 #pragma unroll
                         for (uint32_t h = 0; h < 2; ++h) {
@@ -414,11 +428,10 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                                 uint32_t l = lt;
 #pragma unroll
                                 for (int i = 0; i < kRegQubits; ++i)
-                                    if ((r >> i) & 1u) l |= le[i];
+                                    if ((r >> i) & 1u) l ^= le[i];
                                 dst[l] = a[c];
                             }
                         }
-                        fence_proxy_async();     // generic writes -> the TMA store's reads
                         tc_fence_before();
                         mbar_arrive(&staged[b]);
                         kk[s] += 2;

@@ -152,3 +152,37 @@ def test_chain_producer_piece_addressing():
                     assert d not in seen
                     seen[d] = gl | rowoff[c]
         assert len(seen) == 4096 and all(g == mem_of(d // 8) for d, g in seen.items())
+
+
+def test_chain_staged_swizzle_round_trip():
+    """The chain kernel stages the last op's result at 8-byte word
+    l ^ fold4(l) and its producers read piece i (amplitudes 2i, 2i+1) from
+    16-byte unit i ^ (F >> 1), halves swapped when F = fold4(2i) is odd
+    (chain.cu).  Replayed: every piece comes back in order, and the stores
+    of one warp instruction whose lanes cover the four residues mod 4 hit
+    32 distinct banks over two wavefronts."""
+    fold4 = lambda i: ((i >> 4) ^ (i >> 8) ^ (i >> 12)) & 15   # noqa: E731
+    words = {}
+    for l in range(8192):
+        a = l ^ fold4(l)
+        assert a not in words
+        words[a] = l
+    for lane in range(32):
+        for c in range(128):
+            i = lane + 32 * c
+            f = fold4(2 * lane) ^ fold4(64 * c)
+            assert f == fold4(2 * i)
+            u = i ^ (f >> 1)
+            lo, hi = words[2 * u], words[2 * u + 1]
+            if f & 1:
+                lo, hi = hi, lo
+            assert (lo, hi) == (2 * i, 2 * i + 1)
+    # lanes on positions with residues 0..3 mod 4 (plus one more): conflict-free
+    for lanes in ([0, 1, 2, 3, 7], [4, 9, 6, 11, 12], [8, 1, 10, 3, 2]):
+        banks = {}
+        for ln in range(32):
+            l = sum(1 << lanes[b] for b in range(5) if (ln >> b) & 1) | (1 << 5 if 5 not in lanes else 0)
+            a = l ^ fold4(l)
+            banks.setdefault((2 * a) % 32, 0)
+            banks[(2 * a) % 32] += 1
+        assert max(banks.values()) <= 2
