@@ -18,8 +18,8 @@
 // 64 KB buffers: 16-byte cp.async pieces (TMA bulk copies for runs of
 // >= 4 KB) into a buffer, and, after the last op, the result that the
 // compute warps staged in the buffer (bank-swizzled tile order) back to
-// HBM with 16-byte stores; then the buffer takes the tile three ahead.  A twelfth
-// warp issues the MMAs: a slot's 256 threads arrive on its "A ready"
+// HBM with 16-byte stores; then the buffer takes the tile three ahead.  A
+// twelfth warp issues the MMAs: a slot's 256 threads arrive on its "A ready"
 // barrier after writing A and B and go on to the other slot at once, so an
 // MMA issue that waits for the tensor pipe to drain the other slot's MMAs
 // stalls nobody.  HBM traffic: 16 B per amplitude per pass.
@@ -38,9 +38,10 @@ namespace {
 using namespace ptx;
 
 constexpr int kCompute = 256;                     // thread t converts A / D row t
-constexpr int kProducers = 96;                    // warps 8..10: HBM <-> buffers
+constexpr int kProducerWarps = 3;                // warps 8..10: HBM <-> buffers
+constexpr int kProducers = 32 * kProducerWarps;
 constexpr int kMmaThread = kCompute + kProducers; // warp 11, first lane: MMA issue
-constexpr int kThreads = kCompute + kProducers + 32;
+constexpr int kThreads = kCompute + kProducers + 32;   // 384: up to 168 registers a thread
 constexpr uint32_t kTile = 1u << kTileQubits;
 constexpr uint32_t kBufBytes = kTile * 8u;        // 64 KB: the tile (fp32) or its A operand (bf16 hi | lo)
 constexpr uint32_t kBufs = 3;
@@ -69,16 +70,16 @@ __device__ __forceinline__ uint64_t tile_base(const TilePass& P, uint64_t tile) 
 __device__ __forceinline__ uint32_t fold4(uint32_t i) { return ((i >> 4) ^ (i >> 8) ^ (i >> 12)) & 15u; }
 
 // Barrier 2 over the 96 producer threads.
-__device__ __forceinline__ void producer_sync() { asm volatile("bar.sync 2, 96;" ::: "memory"); }
+__device__ __forceinline__ void producer_sync() { asm volatile("bar.sync 2, %0;" ::"n"(kProducers) : "memory"); }
 __device__ __forceinline__ bool producer_any(bool x) {
     uint32_t r;
     asm volatile(
         "{\n\t.reg .pred p, q;\n\t"
         "setp.ne.u32 p, %1, 0;\n\t"
-        "bar.red.or.pred q, 2, 96, p;\n\t"
+        "bar.red.or.pred q, 2, %2, p;\n\t"
         "selp.u32 %0, 1, 0, q;\n\t}"
         : "=r"(r)
-        : "r"(x ? 1u : 0u)
+        : "r"(x ? 1u : 0u), "n"(kProducers)
         : "memory");
     return r != 0;
 }
@@ -116,31 +117,35 @@ __device__ __forceinline__ void issue_mmas(uint32_t a, uint32_t b, uint32_t d, u
     tc_commit(bar);
 }
 
-// Reads 16 amplitudes (register indices 16 h .. 16 h + 15) of this thread's
-// D row: D1 + D2, columns 32 h .. 32 h + 31 of each.
-__device__ __forceinline__ void read_half(uint32_t row, uint32_t h, float2 (&a)[16]) {
-    uint32_t r1[32], r2[32];
-    tc_ld_32(row + h * 32u, r1);
-    tc_ld_32(row + 64u + h * 32u, r2);
+// Reads 8 amplitudes (register indices 8 q .. 8 q + 7) of this thread's D
+// row: D1 + D2, columns 16 q .. 16 q + 15 of each.
+__device__ __forceinline__ void read_quarter(uint32_t row, uint32_t q, float2 (&a)[8]) {
+    uint32_t r1[16], r2[16];
+    tc_ld_16(row + q * 16u, r1);
+    tc_ld_16(row + 64u + q * 16u, r2);
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int c = 0; c < 16; ++c)
+    for (int c = 0; c < 8; ++c)
         a[c] = make_float2(__uint_as_float(r1[2 * c]) + __uint_as_float(r2[2 * c]),
                            __uint_as_float(r1[2 * c + 1]) + __uint_as_float(r2[2 * c + 1]));
 }
 
-// Scatters amplitudes with register indices base_r .. base_r + 15 into the
-// A operand at `a` (hi; lo 32 KB above): byte offset = thread part ^ XOR of
-// d[i] over the index's set bits.
-__device__ __forceinline__ void scatter16(const float2 (&v)[16], uint32_t base_r, uint32_t thr_off,
-                                          const uint32_t (&d)[kRegQubits], unsigned char* a) {
+// Scatters amplitudes with register indices base_r .. base_r + N - 1 into
+// the A operand at `a` (hi; lo 32 KB above): byte offset = thread part ^
+// XOR of d[i] over the index's set bits.
+template <int N>
+__device__ __forceinline__ void scatter(const float2 (&v)[N], uint32_t base_r, uint32_t thr_off,
+                                        const uint32_t (&d)[kRegQubits], unsigned char* a) {
+    // Gray-code order: one XOR moves the offset to the next amplitude, so no
+    // table of N offsets stays live
+    uint32_t off = thr_off;
 #pragma unroll
-    for (uint32_t c = 0; c < 16; ++c) {
-        const uint32_t r = base_r + c;
-        uint32_t off = thr_off;
+    for (int i = 0; i < kRegQubits; ++i)
+        if ((base_r >> i) & 1u) off ^= d[i];
 #pragma unroll
-        for (int i = 0; i < kRegQubits; ++i)
-            if ((r >> i) & 1u) off ^= d[i];
+    for (uint32_t k = 0; k < N; ++k) {
+        if (k) off ^= d[(k & 1u) ? 0 : (k & 2u) ? 1 : (k & 4u) ? 2 : (k & 8u) ? 3 : 4];   // lowest set bit of k
+        const uint32_t c = k ^ (k >> 1);
         uint32_t hi, lo;
         tc_split(v[c], hi, lo);
         *reinterpret_cast<uint32_t*>(a + off) = hi;
@@ -248,8 +253,8 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
     } else if (tid >= kCompute) {
         // ---- the producer warps: tile k goes into buffer k % 3 after tile
         // k - 3's staged result has been stored from it ------------------------
-        const uint32_t pt = tid - kCompute;            // 0..95
-        const uint32_t lane = pt & 31u, pw = pt >> 5;  // pw: 0..2 takes piece rows c = pw, pw + 3, ...
+        const uint32_t pt = tid - kCompute;            // 0 .. kProducers - 1
+        const uint32_t lane = pt & 31u, pw = pt >> 5;  // warp pw takes piece rows c = pw, pw + 7, ...
         const uint32_t nl = P.n_low;
         float2* __restrict__ state = w.state;
         uint64_t gl = 0;
@@ -268,7 +273,8 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
             const uint4* src = reinterpret_cast<const uint4*>(bufs + b * kBufBytes);
             uint4* dst = reinterpret_cast<uint4*>(state);
             const uint32_t fl = fold4(2u * lane);
-            for (uint32_t c = pw; c < 128; c += 3) {
+#pragma unroll 6
+            for (uint32_t c = pw; c < 128; c += kProducerWarps) {
                 const uint32_t f = fl ^ fold4(64u * c);
                 uint4 v = src[(lane + 32u * c) ^ (f >> 1)];
                 if (f & 1u) v = make_uint4(v.z, v.w, v.x, v.y);
@@ -300,7 +306,8 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
             } else {
                 const uint32_t d0 = smem_u32(buf) + 16u * lane;
                 const uint64_t g0 = base | gl;
-                for (uint32_t c = pw; c < 128; c += 3)
+#pragma unroll 6
+                for (uint32_t c = pw; c < 128; c += kProducerWarps)
                     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d0 + 512u * c),
                                  "l"(state + (g0 | rowoff[c]))
                                  : "memory");
@@ -338,14 +345,18 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                 unsigned char* buf = bufs + b * kBufBytes;
                 unsigned char* bs = bstage + s * kTcBBytes;
                 const uint32_t dcol = tmem + 256u * s;
-                // B of the op this step issues (L2-resident; its load latency
-                // hides behind the wait and the conversion)
-                uint4 bq[kBPerThread];
-                if (j < m) {
-                    const uint4* bsrc = reinterpret_cast<const uint4*>(mats + sboff[first + j]);
+                // B of the op this step issues (L2-resident), copied straight
+                // into the slot's staging once its previous MMAs are done; the
+                // copy lands while the tile is converted
+                auto copy_b = [&]() {
+                    const float2* bsrc = mats + sboff[first + j];
+                    const uint32_t bdst = smem_u32(bs) + 16u * t;
 #pragma unroll
-                    for (uint32_t i = 0; i < kBPerThread; ++i) bq[i] = __ldg(bsrc + i * kCompute + t);
-                }
+                    for (uint32_t i = 0; i < kBPerThread; ++i)
+                        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(bdst + i * 16u * kCompute),
+                                     "l"(bsrc + 2u * (i * kCompute + t))
+                                     : "memory");
+                };
                 if (j == 0) {
                     // the loaded tile -> A of the first op
                     const bool ok = mbar_wait_bounded(&full[b], (kk[s] / kBufs) & 1u);
@@ -354,6 +365,7 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                         if (t == 0) atomicExch(err, 1);
                         break;
                     }
+                    copy_b();
                     const TilePhase& R = sph[0];
                     uint32_t tp = 0, e[kRegQubits];
 #pragma unroll
@@ -382,14 +394,7 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                             if ((t >> i) & 1u) thr ^= F.a_thr[i];
 #pragma unroll
                         for (int i = 0; i < kRegQubits; ++i) d[i] = F.a_reg[i];
-                        float2 h0[16], h1[16];
-#pragma unroll
-                        for (int c = 0; c < 16; ++c) {
-                            h0[c] = v[c];
-                            h1[c] = v[16 + c];
-                        }
-                        scatter16(h0, 0u, thr, d, buf);
-                        scatter16(h1, 16u, thr, d, buf);
+                        scatter<32>(v, 0u, thr, d, buf);
                     }
                 } else {
                     const bool ok = mbar_wait_bounded(&mmab[s], uses[s] & 1u);
@@ -419,12 +424,12 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                         }
                         float2* dst = reinterpret_cast<float2*>(buf);
 #pragma unroll
-                        for (uint32_t h = 0; h < 2; ++h) {
-                            float2 a[16];
-                            read_half(dcol + drow, h, a);
+                        for (uint32_t h = 0; h < 4; ++h) {
+                            float2 a[8];
+                            read_quarter(dcol + drow, h, a);
 #pragma unroll
-                            for (uint32_t c = 0; c < 16; ++c) {
-                                const uint32_t r = 16u * h + c;
+                            for (uint32_t c = 0; c < 8; ++c) {
+                                const uint32_t r = 8u * h + c;
                                 uint32_t l = lt;
 #pragma unroll
                                 for (int i = 0; i < kRegQubits; ++i)
@@ -439,6 +444,7 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                         continue;
                     }
                     // D of op j - 1 -> A of op j
+                    copy_b();
                     const TilePhase& F = sph[first + j];
                     uint32_t thr = 0, d[kRegQubits];
 #pragma unroll
@@ -447,18 +453,15 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
 #pragma unroll
                     for (int i = 0; i < kRegQubits; ++i) d[i] = F.a_reg[i];
 #pragma unroll
-                    for (uint32_t h = 0; h < 2; ++h) {
-                        float2 a[16];
-                        read_half(dcol + drow, h, a);
-                        scatter16(a, 16u * h, thr, d, buf);
+                    for (uint32_t h = 0; h < 4; ++h) {
+                        float2 a[8];
+                        read_quarter(dcol + drow, h, a);
+                        scatter<8>(a, 8u * h, thr, d, buf);
                     }
                 }
-                // B into this slot's staging (its previous MMAs are done), then
                 // A and B go to the tensor core: the MMA warp issues once every
                 // compute thread has arrived
-                uint4* bdst = reinterpret_cast<uint4*>(bs);
-#pragma unroll
-                for (uint32_t i = 0; i < kBPerThread; ++i) bdst[i * kCompute + t] = bq[i];
+                asm volatile("cp.async.wait_all;" ::: "memory");   // this thread's part of B landed
                 if (t == 0) {
                     mbox[4 * s] = smem_u32(buf);
                     mbox[4 * s + 1] = smem_u32(bs);
