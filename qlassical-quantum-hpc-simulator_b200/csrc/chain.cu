@@ -14,12 +14,12 @@
 // tensor-memory columns and its own B staging): while slot 0's MMAs run,
 // the 256 compute threads convert slot 1's tile, and the other way round.
 // Slot 1 starts half a tile behind slot 0, so its buffer's next load has
-// time to land.  Three producer warps move the tiles between HBM and three
+// time to land.  Seven producer warps move the tiles between HBM and three
 // 64 KB buffers: 16-byte cp.async pieces (TMA bulk copies for runs of
 // >= 4 KB) into a buffer, and, after the last op, the result that the
 // compute warps staged in the buffer (bank-swizzled tile order) back to
 // HBM with 16-byte stores; then the buffer takes the tile three ahead.  A
-// twelfth warp issues the MMAs: a slot's 256 threads arrive on its "A ready"
+// sixteenth warp issues the MMAs: a slot's 256 threads arrive on its "A ready"
 // barrier after writing A and B and go on to the other slot at once, so an
 // MMA issue that waits for the tensor pipe to drain the other slot's MMAs
 // stalls nobody.  HBM traffic: 16 B per amplitude per pass.
@@ -38,10 +38,14 @@ namespace {
 using namespace ptx;
 
 constexpr int kCompute = 256;                     // thread t converts A / D row t
-constexpr int kProducerWarps = 3;                // warps 8..10: HBM <-> buffers
+constexpr int kProducerWarps = 7;                // warps 8..14: HBM <-> buffers
 constexpr int kProducers = 32 * kProducerWarps;
-constexpr int kMmaThread = kCompute + kProducers; // warp 11, first lane: MMA issue
-constexpr int kThreads = kCompute + kProducers + 32;   // 384: up to 168 registers a thread
+constexpr int kMmaThread = kCompute + kProducers; // warp 15, first lane: MMA issue
+// 512 threads, 128 registers a thread.  The producers' 16-byte copies are
+// bound by each warp's requests in flight, not by the SM's load/store
+// throughput (a probe of 64-byte-run copies moved about n times as many
+// bytes with n warps up to 16), so the spare warps all copy.
+constexpr int kThreads = kCompute + kProducers + 32;
 constexpr uint32_t kTile = 1u << kTileQubits;
 constexpr uint32_t kBufBytes = kTile * 8u;        // 64 KB: the tile (fp32) or its A operand (bf16 hi | lo)
 constexpr uint32_t kBufs = 3;
