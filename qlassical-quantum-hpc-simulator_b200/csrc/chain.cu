@@ -12,15 +12,14 @@
 // Where the general kernel runs one tile at a time and waits for every
 // MMA, this one keeps two tiles in flight per SM ("slots", each with 256
 // tensor-memory columns and its own B staging): while slot 0's MMAs run,
-// the 512 compute threads (two per A / D row, 16 amplitudes each) convert
-// slot 1's tile, and the other way round.
+// the 256 compute threads convert slot 1's tile, and the other way round.
 // Slot 1 starts half a tile behind slot 0, so its buffer's next load has
-// time to land.  Seven producer warps move the tiles between HBM and three
+// time to land.  Three producer warps move the tiles between HBM and three
 // 64 KB buffers: 16-byte cp.async pieces (TMA bulk copies for runs of
 // >= 4 KB) into a buffer, and, after the last op, the result that the
 // compute warps staged in the buffer (bank-swizzled tile order) back to
 // HBM with 16-byte stores; then the buffer takes the tile three ahead.  A
-// last warp issues the MMAs: a slot's 512 threads arrive on its "A ready"
+// twelfth warp issues the MMAs: a slot's 256 threads arrive on its "A ready"
 // barrier after writing A and B and go on to the other slot at once, so an
 // MMA issue that waits for the tensor pipe to drain the other slot's MMAs
 // stalls nobody.  HBM traffic: 16 B per amplitude per pass.
@@ -38,15 +37,13 @@ namespace {
 
 using namespace ptx;
 
-constexpr int kRows = 256;                        // A / D rows of a tile
-constexpr int kCompute = 2 * kRows;               // thread t converts half (t >> 8) of row t & 255
-constexpr int kProducerWarps = 7;                // warps 16..22: HBM <-> buffers
+constexpr int kCompute = 256;                     // thread t converts A / D row t
+constexpr int kProducerWarps = 3;                // warps 8..10: HBM <-> buffers
 constexpr int kProducers = 32 * kProducerWarps;
-constexpr int kMmaThread = kCompute + kProducers; // warp 23, first lane: MMA issue
-// 768 threads, 80 registers a thread.  The producers' 16-byte copies are
-// bound by each warp's requests in flight, not by the SM's load/store
-// throughput (a probe of 64-byte-run copies moved about n times as many
-// bytes with n warps up to 16), so the spare warps all copy.
+constexpr int kMmaThread = kCompute + kProducers; // warp 11, first lane: MMA issue
+// 384 threads, up to 168 registers a thread.  (Measured on the fused
+// 30-qubit circuit: seven producer warps, at 128 registers, or two compute
+// threads per row, at 80, ran no faster -- the copies keep up with three.)
 constexpr int kThreads = kCompute + kProducers + 32;
 constexpr uint32_t kTile = 1u << kTileQubits;
 constexpr uint32_t kBufBytes = kTile * 8u;        // 64 KB: the tile (fp32) or its A operand (bf16 hi | lo)
@@ -90,17 +87,17 @@ __device__ __forceinline__ bool producer_any(bool x) {
     return r != 0;
 }
 
-// Barrier 1 over the compute threads (the producer and MMA warps never join it).
-__device__ __forceinline__ void compute_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kCompute) : "memory"); }
+// Barrier 1 over the 256 compute threads (the load warp never joins it).
+__device__ __forceinline__ void compute_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 __device__ __forceinline__ bool compute_any(bool x) {
     uint32_t r;
     asm volatile(
         "{\n\t.reg .pred p, q;\n\t"
         "setp.ne.u32 p, %1, 0;\n\t"
-        "bar.red.or.pred q, 1, %2, p;\n\t"
+        "bar.red.or.pred q, 1, 256, p;\n\t"
         "selp.u32 %0, 1, 0, q;\n\t}"
         : "=r"(r)
-        : "r"(x ? 1u : 0u), "n"(kCompute)
+        : "r"(x ? 1u : 0u)
         : "memory");
     return r != 0;
 }
@@ -159,21 +156,6 @@ __device__ __forceinline__ void scatter(const float2 (&v)[N], uint32_t base_r, u
     }
 }
 
-// Writes half hh of A row `row` (hi and lo), identity K order: chunk j holds
-// amplitudes 4j .. 4j + 3 of the row, v[c] = amplitude 16 hh + c.
-__device__ __forceinline__ void write_a_half(const float2 (&v)[16], uint32_t row, uint32_t hh, unsigned char* a) {
-#pragma unroll
-    for (uint32_t q = 0; q < 4; ++q) {
-        const uint32_t j = 4u * hh + q;
-        uint32_t hi[4], lo[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) tc_split(v[4 * q + e], hi[e], lo[e]);
-        const uint32_t off = row * 128u + ((j ^ (row & 7u)) << 4);
-        *reinterpret_cast<uint4*>(a + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-        *reinterpret_cast<uint4*>(a + 32768u + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-    }
-}
-
 __global__ void __launch_bounds__(kThreads, 1)
 k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -216,12 +198,12 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
     if (tid == 0) {
         for (int b = 0; b < 3; ++b) {
             mbar_init(&full[b], kProducers);    // one (deferred) arrival per producer thread
-            mbar_init(&staged[b], kCompute);    // every compute thread, after its writes
+            mbar_init(&staged[b], kCompute / 32);   // every compute warp, after its writes
         }
         mbar_init(&mmab[0], 1);
         mbar_init(&mmab[1], 1);
-        mbar_init(&aready[0], kCompute);
-        mbar_init(&aready[1], kCompute);
+        mbar_init(&aready[0], kCompute / 32);
+        mbar_init(&aready[1], kCompute / 32);
         fence_mbar_init();
     }
     if (tid < 32) {
@@ -342,9 +324,8 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
     } else {
         // ---- the compute warps: two slots, one step each per round -----------
         const uint32_t t = tid;
-        const uint32_t row = t & (kRows - 1u), hh = t / kRows;   // A / D row, half of its amplitudes
         const uint32_t wq = t >> 5;
-        const uint32_t drow = ((wq & 3u) * 32u) << 16 | (((wq >> 2) & 1u) * 128u);   // lane quarter, M-block
+        const uint32_t drow = ((wq & 3u) * 32u) << 16 | ((wq >> 2) * 128u);   // lane quarter, M-block
         uint32_t kk[2] = {0u, 1u};
         int jj[2] = {0, -static_cast<int>((m + 1u) / 2u)};
         uint32_t uses[2] = {0u, 0u};
@@ -392,32 +373,31 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                     uint32_t tp = 0, e[kRegQubits];
 #pragma unroll
                     for (int i = 0; i < kThreadQubits; ++i)
-                        if ((row >> i) & 1u) tp |= 1u << R.thr_pos[i];
-                    if (hh) tp |= 1u << R.reg_pos[4];
+                        if ((t >> i) & 1u) tp |= 1u << R.thr_pos[i];
 #pragma unroll
                     for (int i = 0; i < kRegQubits; ++i) e[i] = 1u << R.reg_pos[i];
                     const float2* src = reinterpret_cast<const float2*>(buf);
-                    float2 v[16];
+                    float2 v[32];
 #pragma unroll
-                    for (int c = 0; c < 16; ++c) {
+                    for (int r = 0; r < 32; ++r) {
                         uint32_t l = tp;
 #pragma unroll
-                        for (int i = 0; i < 4; ++i)
-                            if ((c >> i) & 1) l |= e[i];
-                        v[c] = src[l];
+                        for (int i = 0; i < kRegQubits; ++i)
+                            if ((r >> i) & 1) l |= e[i];
+                        v[r] = src[l];
                     }
                     compute_sync();      // every thread has read the tile: the buffer becomes A
                     if (first == 0) {
-                        write_a_half(v, row, hh, buf);   // own row, identity K order
+                        tc_write_a(v, buf, buf + 32768u);   // own row, identity K order
                     } else {
                         const TilePhase& F = sph[first];
                         uint32_t thr = 0, d[kRegQubits];
 #pragma unroll
                         for (int i = 0; i < kThreadQubits; ++i)
-                            if ((row >> i) & 1u) thr ^= F.a_thr[i];
+                            if ((t >> i) & 1u) thr ^= F.a_thr[i];
 #pragma unroll
                         for (int i = 0; i < kRegQubits; ++i) d[i] = F.a_reg[i];
-                        scatter<16>(v, 16u * hh, thr, d, buf);
+                        scatter<32>(v, 0u, thr, d, buf);
                     }
                 } else {
                     const bool ok = mbar_wait_bounded(&mmab[s], uses[s] & 1u);
@@ -438,7 +418,7 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                         uint32_t lt = 0, le[kRegQubits];
 #pragma unroll
                         for (int i = 0; i < kThreadQubits; ++i)
-                            if ((row >> i) & 1u) lt |= 1u << L.thr_pos[i];
+                            if ((t >> i) & 1u) lt |= 1u << L.thr_pos[i];
                         lt ^= fold4(lt);
 #pragma unroll
                         for (int i = 0; i < kRegQubits; ++i) {
@@ -447,8 +427,7 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                         }
                         float2* dst = reinterpret_cast<float2*>(buf);
 #pragma unroll
-                        for (uint32_t hq = 0; hq < 2; ++hq) {
-                            const uint32_t h = 2u * hh + hq;
+                        for (uint32_t h = 0; h < 4; ++h) {
                             float2 a[8];
                             read_quarter(dcol + drow, h, a);
 #pragma unroll
@@ -462,7 +441,8 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                             }
                         }
                         tc_fence_before();
-                        mbar_arrive(&staged[b]);
+                        __syncwarp();
+                        if ((t & 31u) == 0) mbar_arrive(&staged[b]);   // for the whole warp
                         kk[s] += 2;
                         jj[s] = 0;
                         continue;
@@ -473,12 +453,11 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                     uint32_t thr = 0, d[kRegQubits];
 #pragma unroll
                     for (int i = 0; i < kThreadQubits; ++i)
-                        if ((row >> i) & 1u) thr ^= F.a_thr[i];
+                        if ((t >> i) & 1u) thr ^= F.a_thr[i];
 #pragma unroll
                     for (int i = 0; i < kRegQubits; ++i) d[i] = F.a_reg[i];
 #pragma unroll
-                    for (uint32_t hq = 0; hq < 2; ++hq) {
-                        const uint32_t h = 2u * hh + hq;
+                    for (uint32_t h = 0; h < 4; ++h) {
                         float2 a[8];
                         read_quarter(dcol + drow, h, a);
                         scatter<8>(a, 8u * h, thr, d, buf);
@@ -494,7 +473,8 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                 }
                 fence_proxy_async();
                 tc_fence_before();
-                mbar_arrive(&aready[s]);
+                __syncwarp();
+                if ((t & 31u) == 0) mbar_arrive(&aready[s]);   // for the whole warp
                 pending[s] = true;
                 jj[s] = static_cast<int>(j) + 1;
             }
