@@ -46,10 +46,11 @@ UNIT = "amp-updates/s"
 
 # DRAM bytes (read + write) of one tile pass per algorithmic byte (16 B per
 # amplitude): ncu's dram__bytes_read.sum + dram__bytes_write.sum of one
-# tensor-core pass of the fused rotation circuit at 26 qubits, 1014.7 MB
-# against 1073.7 MB algorithmic.  A pass's traffic grows in proportion to
-# the amplitudes it processes, so full-size launches are scaled by this ratio.
-TRAFFIC_PER_ALGORITHMIC_BYTE = 1014.7 / 1073.7
+# chain pass (k_tc_chain) of the fused rotation circuit at 26 qubits,
+# 1015.6 MB against 1073.7 MB algorithmic.  A pass's traffic grows in
+# proportion to the amplitudes it processes, so full-size launches are
+# scaled by this ratio.
+TRAFFIC_PER_ALGORITHMIC_BYTE = 1015.6 / 1073.7
 
 
 def parse():
@@ -485,7 +486,10 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": TRAFFIC_PER_ALGORITHMIC_BYTE * bytes_per_launch,
                      "traffic_source": "ncu dram bytes of a 26-qubit pass, scaled to 2^n amplitudes",
-                     "kernel": "k_tile_pass", "peak_source": _peak_source()},
+                     "kernel": (f"k_tc_chain ({pstats.get('chain_passes', 0)} of {pstats['launches']} passes), "
+                                f"k_tile_pass (the rest)") if pstats.get("chain_passes", 0) else "k_tile_pass",
+                     "of": "16 B x 2^n per pass / (timed step / launches per step)",
+                     "peak_source": _peak_source()},
         "clocks": clocks,
         "gpu_launches": args.steps * pstats["launches"],
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
