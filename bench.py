@@ -596,7 +596,9 @@ def batched_workload(q, args, rank=0, world=1, mode="auto"):
     from qlassical_b200.batch import run_batch
     ez2 = run_batch(mods, mode)
     e2e_s = time.perf_counter() - t0
-    assert all(np.array_equal(x, y) for x, y in zip(ez, ez2))
+    # the same circuits; under "auto" the search may pick another configuration
+    # (its timings differ run to run), so the results agree to rounding only
+    assert all(np.allclose(x, y, atol=5e-5, rtol=0) for x, y in zip(ez, ez2))
     # sequential plain launches, measured: one engine per size, one circuit at a time
     sample = mods[:256]
     engines = {}
@@ -628,8 +630,15 @@ def batched_workload(q, args, rank=0, world=1, mode="auto"):
                                f"[10, 20], depth U{{8..32}}, <Z_i> per circuit",
                    "circuits": len(mods), "mode": st["mode"], "rounds": st["rounds"], "passes": st["passes"],
                    "amp_updates_per_step": st["amp_updates"], "state_bytes": st["state_bytes"],
-                   "autotune_ms": list(st["autotune_ms"]), "build_s": build_s,
+                   "build_s": build_s,
                    "l2": "4 GB of states, larger than the 126 MB L2"},
+        "autotune": {"candidates": [q._lib.batch_tune_candidate(k) for k in range(q._lib.BATCH_TUNE_CANDIDATES)],
+                     "method": "per size class: each candidate plans a sample of the class; CUDA events around "
+                               "3 runs of the sample's tile rounds; one mode for the batch (a round runs one "
+                               "kernel body), the fastest fixed-low count in it per class",
+                     "search_s": st.get("tune_seconds"),
+                     "rounds_ms_projected": {"chosen": st["autotune_ms"][0], "default": st["autotune_ms"][1]},
+                     "classes": st.get("tune", [])},
         "amp_updates_per_s": st["amp_updates"] / step_s,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": TRAFFIC_PER_ALGORITHMIC_BYTE * bytes_step / max(1, st["rounds"]),

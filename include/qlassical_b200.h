@@ -172,8 +172,12 @@ int qlb_engine_get_mode(qlb_engine_t e, int* mode);
  * over the tile becomes one tensor-core op whatever its cost, and a pass
  * made only of such phases runs on the tensor-core chain kernel (two tiles
  * in flight per SM, loads by a dedicated warp); 0 keeps every pass on the
- * general tile kernel. */
-enum qlb_option { QLB_OPT_PHYSICAL_GLOBAL_SWAP = 1, QLB_OPT_TC_MIN_COST = 2, QLB_OPT_TC_CHAIN = 3 };
+ * general tile kernel.  QLB_OPT_TILE_LOW (tiled modes, 3..6, default 3):
+ * memory qubits 0..value-1 belong to every tile, so a tile is read and
+ * written in contiguous runs of 2^value amplitudes; the other 13 - value
+ * tile qubits are chosen per pass.  The batched autotuner searches it. */
+enum qlb_option { QLB_OPT_PHYSICAL_GLOBAL_SWAP = 1, QLB_OPT_TC_MIN_COST = 2, QLB_OPT_TC_CHAIN = 3,
+                  QLB_OPT_TILE_LOW = 4 };
 int qlb_engine_set_option(qlb_engine_t e, int key, int64_t value);
 int qlb_engine_synchronize(qlb_engine_t e);
 /* The device state pointer (float2 *) and the stream the engine launches on. */
@@ -211,6 +215,12 @@ int qlb_plan_destroy(qlb_plan_t plan);
 int qlb_describe_plan(uint32_t num_qubits, int mode, int physical_global_swap,
                       const qlb_gate_instr* program, uint64_t count, const qlb_pool_view* pool,
                       char* out, uint64_t cap, uint64_t* needed);
+/* The same with the planner options an engine takes from QLB_OPT_TILE_LOW
+ * (tile_low, 3..6) and QLB_OPT_TC_CHAIN (tc_chain); qlb_describe_plan is
+ * tile_low 3, tc_chain 1. */
+int qlb_describe_plan_opts(uint32_t num_qubits, int mode, int physical_global_swap, int tile_low, int tc_chain,
+                           const qlb_gate_instr* program, uint64_t count, const qlb_pool_view* pool,
+                           char* out, uint64_t cap, uint64_t* needed);
 
 /* FP64 reductions over the device state (no reference counterpart except
  * the probability reduction inside apply_measure, :622-630). */
@@ -310,23 +320,48 @@ int qlb_gpu_safe_qubit_limit(uint32_t* out);
 
 typedef struct qlb_batch* qlb_batch_t;
 
+/* The batched autotuner (mode -1) times QLB_BATCH_TUNE_CANDIDATES planner
+ * configurations per size class -- the circuits of one padded qubit count,
+ * 13..30: candidate i runs mode QLB_MODE_TILED (i < 3) or QLB_MODE_TILED_TC
+ * (i >= 3) with 3 + i % 3 fixed low tile qubits (QLB_OPT_TILE_LOW), each on
+ * a sample of the class (its first circuits, about two tiles per SM, at most
+ * 128) by CUDA events around three runs of the sample's tile rounds.  A
+ * round launches one kernel body for all its passes, so the mode is chosen
+ * for the whole batch (the smaller total of the classes' best candidates in
+ * that mode, projected to the class sizes) and the fixed low qubits per
+ * class. */
+#define QLB_BATCH_TUNE_CANDIDATES 6
+#define QLB_BATCH_TUNE_CLASSES 18
+typedef struct qlb_batch_tune_class {
+    uint32_t num_qubits;    /* padded qubit count (13..30) */
+    uint32_t circuits;      /* circuits of the class in the batch */
+    uint32_t sample;        /* circuits timed per candidate */
+    int32_t  best;          /* the candidate that plans the class (in the batch's mode) */
+    float    ms[QLB_BATCH_TUNE_CANDIDATES];  /* sample time per candidate; < 0: the candidate failed to plan */
+} qlb_batch_tune_class;
+
 typedef struct qlb_batch_info {
     uint32_t circuits;
     uint32_t rounds;        /* tile-kernel launches = max passes over the circuits */
-    int      mode;          /* the mode in use (the autotuner's pick for mode -1) */
+    int      mode;          /* QLB_MODE_TILED or QLB_MODE_TILED_TC; -1: size classes differ */
     uint32_t launches;      /* kernel launches per run */
     uint64_t tiles;         /* 2^13-amplitude tiles processed per run */
     uint64_t passes;        /* sum over circuits of executed passes */
     uint64_t amp_updates;   /* sum over circuits of (gates * 2^num_qubits) */
     uint64_t state_bytes;   /* device bytes of all state vectors */
-    double   autotune_ms[2];/* mode -1: one run with TILED, with TILED_TC */
+    double   autotune_ms[2];/* mode -1: the tile rounds of the whole batch projected from the
+                               samples: [0] the chosen configuration, [1] candidate 0 everywhere */
+    double   tune_seconds;  /* mode -1: host time of the search (sample planning and timing) */
+    uint32_t tune_classes;  /* mode -1: entries of tune[] in use */
+    uint32_t pad;
+    qlb_batch_tune_class tune[QLB_BATCH_TUNE_CLASSES];
 } qlb_batch_info;
 
 /* Plans `count` circuits (program c: counts[c] instructions over pools[c],
  * num_qubits[c] in 1..30; gates only -- no MEASURE or 6-qubit blocks),
  * allocates every state vector and captures one CUDA graph per run.
- * mode: QLB_MODE_TILED, QLB_MODE_TILED_TC, or -1 to time both and keep the
- * faster. */
+ * mode: QLB_MODE_TILED, QLB_MODE_TILED_TC (3 fixed low tile qubits), or -1
+ * to autotune each size class (above). */
 int qlb_batch_create(qlb_batch_t* out, uint32_t count, const qlb_gate_instr* const* programs,
                      const uint64_t* counts, const qlb_pool_view* pools, const uint32_t* num_qubits,
                      int mode);

@@ -47,6 +47,14 @@ MODE_PLAIN = 0
 MODE_TILED = 1
 MODE_TILED_TC = 2
 
+OPT_PHYSICAL_GLOBAL_SWAP = 1
+OPT_TC_MIN_COST = 2
+OPT_TC_CHAIN = 3
+OPT_TILE_LOW = 4
+
+BATCH_TUNE_CANDIDATES = 6
+BATCH_TUNE_CLASSES = 18
+
 
 class QlbError(RuntimeError):
     """A CUDA / device failure reported by the library."""
@@ -89,6 +97,21 @@ class ExecStats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class BatchTuneClass(ctypes.Structure):
+    _fields_ = [
+        ("num_qubits", ctypes.c_uint32),
+        ("circuits", ctypes.c_uint32),
+        ("sample", ctypes.c_uint32),
+        ("best", ctypes.c_int32),
+        ("ms", ctypes.c_float * BATCH_TUNE_CANDIDATES),
+    ]
+
+
+def batch_tune_candidate(i: int) -> dict:
+    """Candidate i of the batched autotuner (qlb_batch_tune_class)."""
+    return {"mode": "tiled" if i < 3 else "tiled_tc", "tile_low": 3 + i % 3}
+
+
 class BatchInfo(ctypes.Structure):
     _fields_ = [
         ("circuits", ctypes.c_uint32),
@@ -100,6 +123,10 @@ class BatchInfo(ctypes.Structure):
         ("amp_updates", ctypes.c_uint64),
         ("state_bytes", ctypes.c_uint64),
         ("autotune_ms", ctypes.c_double * 2),
+        ("tune_seconds", ctypes.c_double),
+        ("tune_classes", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
+        ("tune", BatchTuneClass * BATCH_TUNE_CLASSES),
     ]
 
 
@@ -131,6 +158,13 @@ class Check64Result(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+# qlb_cost_model_fn: (ctx, window_frequencies, log_to_phys, phys_to_log,
+# num_qubits, *active, *victim) -> 1 to request a swap, 0 for none.
+COST_MODEL_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
+                                 ctypes.POINTER(ctypes.c_uint16), ctypes.POINTER(ctypes.c_uint16), ctypes.c_uint32,
+                                 ctypes.POINTER(ctypes.c_uint16), ctypes.POINTER(ctypes.c_uint16))
+
+
 class TranspileConfig(ctypes.Structure):
     _fields_ = [
         ("enable_gate_fusion", ctypes.c_int),
@@ -141,6 +175,8 @@ class TranspileConfig(ctypes.Structure):
         ("k_safe", ctypes.c_int),
         ("max_fusion_qubits", ctypes.c_int),
         ("reference_fusable_set", ctypes.c_int),
+        ("custom_cost_model", COST_MODEL_FN),
+        ("custom_cost_model_ctx", ctypes.c_void_p),
     ]
 
 

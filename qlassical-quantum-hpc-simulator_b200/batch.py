@@ -4,9 +4,12 @@ Each circuit runs from |0...0> and reports <Z_q> for its qubits (FP64
 reduction), exactly as CUDAEngine.execute() followed by expect_z() would,
 but all circuits advance together: one tile-kernel launch per pass round
 over a work list of (state, pass) entries, captured with the |0...0>
-set-up and the reductions into one CUDA graph.  ``mode="auto"`` plans the
-batch both with FP32 CUDA-core tiles and with tensor-core fused tiles,
-times one run of each, and keeps the faster.
+set-up and the reductions into one CUDA graph.  ``mode="auto"`` autotunes:
+six planner configurations -- FP32 CUDA-core or tensor-core fused tiles,
+times 3, 4 or 5 fixed low tile qubits -- are timed on a sample of each size
+class (circuits of one padded qubit count); the mode is chosen for the whole
+batch (a round runs one kernel body) and the fixed low qubits per class;
+``stats()["tune"]`` reports the search.
 """
 from __future__ import annotations
 
@@ -20,7 +23,7 @@ from ._lib import call, lib
 from .ir import IRModule
 
 _MODES = {"tiled": _lib.MODE_TILED, "tiled_tc": _lib.MODE_TILED_TC, "auto": -1}
-_MODE_NAMES = {_lib.MODE_TILED: "tiled", _lib.MODE_TILED_TC: "tiled_tc"}
+_MODE_NAMES = {_lib.MODE_TILED: "tiled", _lib.MODE_TILED_TC: "tiled_tc", -1: "per size class"}
 
 
 class Batch:
@@ -88,6 +91,11 @@ class Batch:
             "launches": info.launches, "tiles": info.tiles, "passes": info.passes,
             "amp_updates": info.amp_updates, "state_bytes": info.state_bytes,
             "autotune_ms": list(info.autotune_ms),
+            "tune_seconds": info.tune_seconds,
+            "tune": [{"num_qubits": t.num_qubits, "circuits": t.circuits, "sample": t.sample,
+                      "best": _lib.batch_tune_candidate(t.best),
+                      "ms": [round(float(x), 4) for x in t.ms]}
+                     for t in info.tune[:info.tune_classes]],
         }
 
     def stream(self) -> int:

@@ -8,11 +8,14 @@
 // occupying a launch.  |0...0> set-up, all rounds and the FP64 <Z_i>
 // reduction are captured once into a CUDA graph; qlb_batch_run() is one
 // graph launch.  Circuits below 13 qubits run padded to one 13-qubit tile
-// (the extra qubits stay |0>).  With mode -1 the batch is planned both ways
-// (FP32 CUDA-core tiles and tensor-core fused tiles), each graph is timed
-// once, and the faster one is kept.
+// (the extra qubits stay |0>).  With mode -1 an autotuner times planner
+// configurations -- FP32 CUDA-core tiles or tensor-core fused tiles, 3..5
+// fixed low tile qubits -- on a sample of each size class (circuits of one
+// padded qubit count), then picks the mode for the batch and the fixed low
+// qubits per class.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cstring>
 #include <memory>
 #include <thread>
@@ -36,6 +39,7 @@ struct BatchRound {
     uint32_t n_work;
     uint64_t tiles;
     int features;
+    size_t tmap_off;     // byte offset of its tile -> work-entry table (u32 per tile)
 };
 
 // One mode's device program and graph over the shared state buffer.
@@ -66,7 +70,9 @@ struct qlb_batch {
     PinnedBuffer host_result, host_err;
     size_t o_states = 0, o_chunks = 0;
     std::unique_ptr<BatchProgram> prog;
-    float autotune_ms[2] = {0.f, 0.f};
+    double autotune_ms[2] = {0.0, 0.0};
+    double tune_seconds = 0.0;
+    std::vector<qlb_batch_tune_class> tune;
     ~qlb_batch() {
         prog.reset();
         if (stream) cudaStreamDestroy(stream);
@@ -75,45 +81,69 @@ struct qlb_batch {
 
 namespace {
 
-std::unique_ptr<BatchProgram> build_program(qlb_batch& b, int mode, const qlb_gate_instr* const* programs,
-                                            const uint64_t* counts, const qlb_pool_view* pools) {
-    const uint32_t C = b.count;
-    std::vector<HostPlan> plans(C);
-    {
-        std::atomic<uint32_t> next{0};
-        std::vector<std::string> errs(C);
-        std::vector<int> codes(C, 0);
-        auto worker = [&] {
-            for (uint32_t c; (c = next.fetch_add(1)) < C;) {
-                try {
-                    const PlanConfig cfg{b.states[c].eff_qubits, mode, 0, 10.0, 0};   // work lists: no chain kernel
-                    plans[c] = plan_host(cfg, programs[c], counts[c], &pools[c]);
-                } catch (const Error& e) {
-                    codes[c] = e.code;
-                    errs[c] = e.msg;
-                }
+// A planner configuration the autotuner can pick (qlb_batch_tune_class).
+struct TuneCand {
+    int mode;
+    int tile_low;
+};
+TuneCand tune_candidate(int i) { return TuneCand{i < 3 ? QLB_MODE_TILED : QLB_MODE_TILED_TC, kTileLow + i % 3}; }
+
+struct PlanJob {
+    uint32_t circuit;
+    int cand;
+};
+
+// Plans every job (one circuit under one candidate) on host threads.
+std::vector<HostPlan> plan_jobs(const qlb_batch& b, const std::vector<PlanJob>& jobs,
+                                const qlb_gate_instr* const* programs, const uint64_t* counts,
+                                const qlb_pool_view* pools) {
+    const size_t J = jobs.size();
+    std::vector<HostPlan> plans(J);
+    std::atomic<size_t> next{0};
+    std::vector<std::string> errs(J);
+    std::vector<int> codes(J, 0);
+    auto worker = [&] {
+        for (size_t j; (j = next.fetch_add(1)) < J;) {
+            const uint32_t c = jobs[j].circuit;
+            const TuneCand tc = tune_candidate(jobs[j].cand);
+            try {
+                // work lists run on the general tile kernel: no chain passes
+                const PlanConfig cfg{b.states[c].eff_qubits, tc.mode, 0, 10.0, 0, tc.tile_low};
+                plans[j] = plan_host(cfg, programs[c], counts[c], &pools[c]);
+            } catch (const Error& e) {
+                codes[j] = e.code;
+                errs[j] = e.msg;
             }
-        };
-        unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-        nt = std::min<unsigned>(nt, C);
-        std::vector<std::thread> th;
-        for (unsigned i = 1; i < nt; ++i) th.emplace_back(worker);
-        worker();
-        for (auto& t : th) t.join();
-        for (uint32_t c = 0; c < C; ++c)
-            if (codes[c]) fail(static_cast<qlb_status>(codes[c]), "circuit " + std::to_string(c) + ": " + errs[c]);
-    }
+        }
+    };
+    unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    nt = static_cast<unsigned>(std::min<size_t>(nt, J));
+    std::vector<std::thread> th;
+    for (unsigned i = 1; i < nt; ++i) th.emplace_back(worker);
+    worker();
+    for (auto& t : th) t.join();
+    for (size_t j = 0; j < J; ++j)
+        if (codes[j])
+            fail(static_cast<qlb_status>(codes[j]), "circuit " + std::to_string(jobs[j].circuit) + ": " + errs[j]);
+    return plans;
+}
+
+// Merges the plans of `members` (plans[i] belongs to members[i]) into one
+// device program of rounds over the shared state buffer.
+std::unique_ptr<BatchProgram> assemble(qlb_batch& b, const std::vector<uint32_t>& members,
+                                       std::vector<HostPlan>& plans, int mode) {
+    const size_t C = members.size();
     // merge
     auto P = std::make_unique<BatchProgram>();
     P->mode = mode;
     TileProgram all;
     std::vector<std::vector<uint32_t>> pass_ids(C);
     size_t max_passes = 0;
-    for (uint32_t c = 0; c < C; ++c) {
-        HostPlan& h = plans[c];
+    for (size_t i = 0; i < C; ++i) {
+        HostPlan& h = plans[i];
         for (const PlanStep& st : h.steps)
             if (st.kind != STEP_PASS)
-                fail(QLB_ERR_INVALID_ARG, "circuit " + std::to_string(c) +
+                fail(QLB_ERR_INVALID_ARG, "circuit " + std::to_string(members[i]) +
                                               ": batched circuits may hold only gates (no MEASURE, no 6-qubit "
                                               "blocks, no physical GLOBAL_SWAP)");
         if (all.mats.size() & 1) all.mats.push_back(make_float2(0.f, 0.f));
@@ -136,21 +166,25 @@ std::unique_ptr<BatchProgram> build_program(qlb_batch& b, int mode, const qlb_ga
             all.ops.push_back(op);
         }
         all.mats.insert(all.mats.end(), h.prog.mats.begin(), h.prog.mats.end());
-        for (const PlanStep& st : h.steps) pass_ids[c].push_back(pb + st.index);
-        max_passes = std::max(max_passes, pass_ids[c].size());
-        P->passes += pass_ids[c].size();
+        for (const PlanStep& st : h.steps) pass_ids[i].push_back(pb + st.index);
+        max_passes = std::max(max_passes, pass_ids[i].size());
+        P->passes += pass_ids[i].size();
     }
     // rounds: the r-th pass of every circuit that has one
     std::vector<TileWork> work;
+    std::vector<uint32_t> tmap;
     for (size_t r = 0; r < max_passes; ++r) {
-        BatchRound R{work.size() * sizeof(TileWork), 0, 0, 0};
-        for (uint32_t c = 0; c < C; ++c) {
-            if (r >= pass_ids[c].size()) continue;
-            const uint32_t pid = pass_ids[c][r];
+        BatchRound R{work.size() * sizeof(TileWork), 0, 0, 0, tmap.size() * sizeof(uint32_t)};
+        for (size_t i = 0; i < C; ++i) {
+            if (r >= pass_ids[i].size()) continue;
+            const uint32_t c = members[i];
+            const uint32_t pid = pass_ids[i][r];
             work.push_back(TileWork{nullptr, R.tiles, nullptr, nullptr, nullptr, nullptr, pid, 0});
             // state pointers are filled in below, once the buffer exists
             work.back().pad = c;
-            R.tiles += uint64_t{1} << (b.states[c].eff_qubits - kTileQubits);
+            const uint64_t nt = uint64_t{1} << (b.states[c].eff_qubits - kTileQubits);
+            tmap.insert(tmap.end(), nt, R.n_work);
+            R.tiles += nt;
             R.n_work += 1;
             R.features |= all.passes[pid].features;
         }
@@ -162,7 +196,8 @@ std::unique_ptr<BatchProgram> build_program(qlb_batch& b, int mode, const qlb_ga
     P->o_ops = align256(P->o_phase + all.phases.size() * sizeof(TilePhase));
     P->o_mat = align256(P->o_ops + all.ops.size() * sizeof(TileOp));
     const size_t o_work = align256(P->o_mat + all.mats.size() * sizeof(float2));
-    const size_t total = align256(o_work + work.size() * sizeof(TileWork));
+    const size_t o_tmap = align256(o_work + work.size() * sizeof(TileWork));
+    const size_t total = align256(o_tmap + tmap.size() * sizeof(uint32_t));
     char* d = static_cast<char*>(P->dev.ensure(total));
     float2* base = static_cast<float2*>(b.state_buf.p);
     for (TileWork& w : work) {
@@ -179,8 +214,16 @@ std::unique_ptr<BatchProgram> build_program(qlb_batch& b, int mode, const qlb_ga
     std::memcpy(h.data() + P->o_ops, all.ops.data(), all.ops.size() * sizeof(TileOp));
     std::memcpy(h.data() + P->o_mat, all.mats.data(), all.mats.size() * sizeof(float2));
     std::memcpy(h.data() + o_work, work.data(), work.size() * sizeof(TileWork));
-    for (BatchRound& R : P->rounds) R.work_off += o_work;
-    check_cuda(cudaMemcpy(d, h.data(), total, cudaMemcpyHostToDevice), "batch program upload");
+    std::memcpy(h.data() + o_tmap, tmap.data(), tmap.size() * sizeof(uint32_t));
+    for (BatchRound& R : P->rounds) {
+        R.work_off += o_work;
+        R.tmap_off += o_tmap;
+    }
+    // On the batch's stream: it does not synchronise with the legacy default
+    // stream, and a cudaMemcpy from pageable memory may return before its DMA
+    // has landed, so a launch on the batch's stream could read the program early.
+    check_cuda(cudaMemcpyAsync(d, h.data(), total, cudaMemcpyHostToDevice, b.stream), "batch program upload");
+    check_cuda(cudaStreamSynchronize(b.stream), "batch program upload");
     return P;
 }
 
@@ -198,7 +241,8 @@ void capture(qlb_batch& b, BatchProgram& P) {
     if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), s);
     for (const BatchRound& R : P.rounds) {
         if (e != cudaSuccess) break;
-        e = launch_tile_work(reinterpret_cast<const TileWork*>(d + R.work_off), R.n_work, R.tiles, R.features, err, s);
+        e = launch_tile_work(reinterpret_cast<const TileWork*>(d + R.work_off), R.n_work, R.tiles, R.features, err, s, 0,
+                             reinterpret_cast<const uint32_t*>(d + R.tmap_off));
     }
     if (e == cudaSuccess)
         e = launch_batch_expect_z(base, st, b.count, chunks, b.chunk_begin.back(), static_cast<double*>(b.partial.p),
@@ -215,22 +259,161 @@ void capture(qlb_batch& b, BatchProgram& P) {
     check_cuda(cudaGraphInstantiate(&P.exec, g, 0), "graph instantiate");
 }
 
-float time_graph(qlb_batch& b, BatchProgram& P) {
-    check_cuda(cudaGraphLaunch(P.exec, b.stream), "graph launch");   // warm
+// Milliseconds of one run of a program's tile rounds (no set-up, no
+// reductions): one warm run, then the mean of `reps` runs between events.
+float time_rounds(qlb_batch& b, const BatchProgram& P, int reps) {
+    check_cuda(configure_tile_kernel(), "tile kernel attributes");
+    const char* d = static_cast<const char*>(P.dev.p);
+    int* err = static_cast<int*>(b.err.p);
+    cudaStream_t s = b.stream;
+    auto rounds = [&]() -> cudaError_t {
+        for (const BatchRound& R : P.rounds) {
+            const cudaError_t e =
+                launch_tile_work(reinterpret_cast<const TileWork*>(d + R.work_off), R.n_work, R.tiles, R.features, err,
+                                 s, 0, reinterpret_cast<const uint32_t*>(d + R.tmap_off));
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    };
     cudaEvent_t t0, t1;
     check_cuda(cudaEventCreate(&t0), "event");
     check_cuda(cudaEventCreate(&t1), "event");
-    cudaEventRecord(t0, b.stream);
-    cudaError_t e = cudaGraphLaunch(P.exec, b.stream);
-    cudaEventRecord(t1, b.stream);
+    cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), s);
+    if (e == cudaSuccess) e = rounds();
+    if (e == cudaSuccess) e = cudaEventRecord(t0, s);
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) e = rounds();
+    if (e == cudaSuccess) e = cudaEventRecord(t1, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b.host_err.p, err, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaEventSynchronize(t1);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     float ms = 0.f;
     if (e == cudaSuccess) cudaEventElapsedTime(&ms, t0, t1);
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
-    check_cuda(e, "autotune run");
+    check_cuda(e, "autotune rounds");
     if (*static_cast<int*>(b.host_err.p) != 0) fail(QLB_ERR_TIMEOUT, "a tile-kernel wait gave up during autotuning");
-    return ms;
+    return ms / static_cast<float>(reps);
+}
+
+// The autotuner: for each size class, plans a sample of its circuits under
+// every candidate, times the sample's rounds, and returns the candidate of
+// each circuit (the fastest of its class).
+std::vector<int> autotune(qlb_batch& b, const qlb_gate_instr* const* programs, const uint64_t* counts,
+                          const qlb_pool_view* pools) {
+    constexpr uint32_t kMaxSample = 128;
+    const uint64_t target_tiles = 2 * static_cast<uint64_t>(sm_count());
+    std::vector<std::vector<uint32_t>> cls(kBatchMaxQubits + 1);
+    for (uint32_t c = 0; c < b.count; ++c) cls[b.states[c].eff_qubits].push_back(c);
+    struct Sample {
+        uint32_t ne;
+        std::vector<uint32_t> members;
+    };
+    std::vector<Sample> samples;
+    std::vector<PlanJob> jobs;
+    for (uint32_t ne = kBatchMinQubits; ne <= kBatchMaxQubits; ++ne) {
+        if (cls[ne].empty()) continue;
+        const uint64_t per = uint64_t{1} << (ne - kTileQubits);
+        const uint64_t want = std::max<uint64_t>(1, (target_tiles + per - 1) / per);
+        const size_t n = static_cast<size_t>(std::min<uint64_t>({want, kMaxSample, cls[ne].size()}));
+        samples.push_back(Sample{ne, std::vector<uint32_t>(cls[ne].begin(), cls[ne].begin() + static_cast<long>(n))});
+        for (int k = 0; k < QLB_BATCH_TUNE_CANDIDATES; ++k)
+            for (uint32_t c : samples.back().members) jobs.push_back(PlanJob{c, k});
+    }
+    if (samples.size() > QLB_BATCH_TUNE_CLASSES) fail(QLB_ERR_INVALID_ARG, "too many size classes");
+    // Candidates that cannot plan a circuit are left out of its class's
+    // search; every circuit plans under candidate 0, the engines' default.
+    std::vector<HostPlan> plans(jobs.size());
+    std::vector<char> planned(jobs.size(), 1);
+    try {
+        plans = plan_jobs(b, jobs, programs, counts, pools);
+    } catch (const Error&) {
+        for (size_t j = 0; j < jobs.size(); ++j) {
+            try {
+                std::vector<PlanJob> one{jobs[j]};
+                plans[j] = std::move(plan_jobs(b, one, programs, counts, pools)[0]);
+            } catch (const Error&) {
+                if (jobs[j].cand == 0) throw;
+                planned[j] = 0;
+            }
+        }
+    }
+    // valid, uniform states for timing
+    check_cuda(cudaMemsetAsync(b.state_buf.p, 0, b.total_amps * sizeof(float2), b.stream), "autotune state");
+    check_cuda(launch_set_basis(static_cast<float2*>(b.state_buf.p),
+                                reinterpret_cast<const BatchState*>(static_cast<const char*>(b.meta.p) + b.o_states),
+                                b.count, b.stream),
+               "autotune basis");
+    std::vector<int> choice(b.count, 0);
+    b.tune.clear();
+    b.autotune_ms[0] = b.autotune_ms[1] = 0.0;
+    size_t j = 0;
+    for (const Sample& S : samples) {
+        qlb_batch_tune_class T{};
+        T.num_qubits = S.ne;
+        T.circuits = static_cast<uint32_t>(cls[S.ne].size());
+        T.sample = static_cast<uint32_t>(S.members.size());
+        T.best = 0;
+        for (int k = 0; k < QLB_BATCH_TUNE_CANDIDATES; ++k) {
+            const size_t n = S.members.size();
+            bool ok = true;
+            for (size_t i = 0; i < n; ++i) ok = ok && planned[j + i];
+            if (ok) {
+                std::vector<HostPlan> part(std::make_move_iterator(plans.begin() + static_cast<long>(j)),
+                                           std::make_move_iterator(plans.begin() + static_cast<long>(j + n)));
+                auto P = assemble(b, S.members, part, tune_candidate(k).mode);
+                T.ms[k] = time_rounds(b, *P, 3);
+            } else {
+                T.ms[k] = -1.f;
+            }
+            j += n;
+        }
+        b.tune.push_back(T);
+    }
+    // A round launches one kernel body for all its passes (the union of
+    // their needs), so a tensor-core class would move every round it shares
+    // onto the tensor-core body: the mode is chosen for the whole batch, by
+    // the smaller projected total of the classes' best candidates in that
+    // mode, and the fixed low qubits per class.
+    auto best_in = [](const qlb_batch_tune_class& T, int mode_index) {
+        int best = -1;
+        for (int k = 3 * mode_index; k < 3 * mode_index + 3; ++k)
+            if (T.ms[k] >= 0.f && (best < 0 || T.ms[k] < T.ms[best])) best = k;
+        return best;
+    };
+    double total[2] = {0.0, 0.0};
+    bool usable[2] = {true, true};
+    for (const qlb_batch_tune_class& T : b.tune) {
+        const double scale = static_cast<double>(T.circuits) / static_cast<double>(T.sample);
+        for (int m = 0; m < 2; ++m) {
+            const int k = best_in(T, m);
+            if (k < 0) usable[m] = false;
+            else total[m] += scale * T.ms[k];
+        }
+        b.autotune_ms[1] += scale * T.ms[0];
+    }
+    const int mode_index = usable[1] && (!usable[0] || total[1] < total[0]) ? 1 : 0;
+    b.autotune_ms[0] = total[mode_index];
+    for (size_t i = 0; i < b.tune.size(); ++i) {
+        b.tune[i].best = best_in(b.tune[i], mode_index);
+        for (uint32_t c : cls[samples[i].ne]) choice[c] = b.tune[i].best;
+    }
+    return choice;
+}
+
+// Plans every circuit under its candidate and assembles the batch program.
+std::unique_ptr<BatchProgram> build_program(qlb_batch& b, const std::vector<int>& choice,
+                                            const qlb_gate_instr* const* programs, const uint64_t* counts,
+                                            const qlb_pool_view* pools) {
+    std::vector<PlanJob> jobs(b.count);
+    std::vector<uint32_t> members(b.count);
+    int mode = tune_candidate(choice[0]).mode;
+    for (uint32_t c = 0; c < b.count; ++c) {
+        jobs[c] = PlanJob{c, choice[c]};
+        members[c] = c;
+        if (tune_candidate(choice[c]).mode != mode) mode = -1;
+    }
+    std::vector<HostPlan> plans = plan_jobs(b, jobs, programs, counts, pools);
+    return assemble(b, members, plans, mode);
 }
 
 }  // namespace
@@ -277,29 +460,27 @@ int qlb_batch_create(qlb_batch_t* out, uint32_t count, const qlb_gate_instr* con
         b->o_chunks = align256(count * sizeof(BatchState));
         const size_t meta_bytes = b->o_chunks + (count + 1) * sizeof(uint64_t);
         char* m = static_cast<char*>(b->meta.ensure(meta_bytes));
-        check_cuda(cudaMemcpy(m + b->o_states, b->states.data(), count * sizeof(BatchState), cudaMemcpyHostToDevice),
+        check_cuda(cudaMemcpyAsync(m + b->o_states, b->states.data(), count * sizeof(BatchState),
+                                   cudaMemcpyHostToDevice, b->stream),
                    "batch states");
-        check_cuda(cudaMemcpy(m + b->o_chunks, b->chunk_begin.data(), (count + 1) * sizeof(uint64_t),
-                              cudaMemcpyHostToDevice),
+        check_cuda(cudaMemcpyAsync(m + b->o_chunks, b->chunk_begin.data(), (count + 1) * sizeof(uint64_t),
+                                   cudaMemcpyHostToDevice, b->stream),
                    "batch chunks");
+        check_cuda(cudaStreamSynchronize(b->stream), "batch metadata upload");
         b->partial.ensure(batch_partial_doubles(chunks) * sizeof(double));
         b->result.ensure(static_cast<size_t>(count) * kBatchStride * sizeof(double));
         b->err.ensure(256);
         b->host_result.ensure(static_cast<size_t>(count) * kBatchStride * sizeof(double));
         b->host_err.ensure(sizeof(int));
         *static_cast<int*>(b->host_err.p) = 0;
+        std::vector<int> choice(count, mode == QLB_MODE_TILED_TC ? 3 : 0);
         if (mode == -1) {
-            auto p0 = build_program(*b, QLB_MODE_TILED, programs, counts, pools);
-            capture(*b, *p0);
-            b->autotune_ms[0] = time_graph(*b, *p0);
-            auto p1 = build_program(*b, QLB_MODE_TILED_TC, programs, counts, pools);
-            capture(*b, *p1);
-            b->autotune_ms[1] = time_graph(*b, *p1);
-            b->prog = b->autotune_ms[1] < b->autotune_ms[0] ? std::move(p1) : std::move(p0);
-        } else {
-            b->prog = build_program(*b, mode, programs, counts, pools);
-            capture(*b, *b->prog);
+            const auto t0 = std::chrono::steady_clock::now();
+            choice = autotune(*b, programs, counts, pools);
+            b->tune_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         }
+        b->prog = build_program(*b, choice, programs, counts, pools);
+        capture(*b, *b->prog);
         *out = b.release();
     });
 }
@@ -366,6 +547,9 @@ int qlb_batch_stats(qlb_batch_t b, qlb_batch_info* out) {
         out->state_bytes = b->total_amps * sizeof(float2);
         out->autotune_ms[0] = b->autotune_ms[0];
         out->autotune_ms[1] = b->autotune_ms[1];
+        out->tune_seconds = b->tune_seconds;
+        out->tune_classes = static_cast<uint32_t>(b->tune.size());
+        for (size_t i = 0; i < b->tune.size() && i < QLB_BATCH_TUNE_CLASSES; ++i) out->tune[i] = b->tune[i];
     });
 }
 

@@ -201,7 +201,7 @@ void check_device_error(qlb_engine& e) {
     int flag = 0;
     check_cuda(cudaMemcpy(&flag, e.err_flag.p, sizeof(int), cudaMemcpyDeviceToHost), "read error flag");
     if (flag != 0) {
-        check_cuda(cudaMemset(e.err_flag.p, 0, sizeof(int)), "clear error flag");
+        check_cuda(cudaMemsetAsync(e.err_flag.p, 0, sizeof(int), e.stream), "clear error flag");
         fail(QLB_ERR_TIMEOUT, "a tile pass gave up waiting for its TMA copies; the state is undefined");
     }
 }
@@ -632,12 +632,18 @@ int qlb_engine_run(qlb_engine_t e, qlb_plan_t plan) {
 
 int qlb_describe_plan(uint32_t n, int mode, int physical, const qlb_gate_instr* prog, uint64_t count,
                       const qlb_pool_view* pool, char* out, uint64_t cap, uint64_t* needed) {
+    return qlb_describe_plan_opts(n, mode, physical, kTileLow, 1, prog, count, pool, out, cap, needed);
+}
+
+int qlb_describe_plan_opts(uint32_t n, int mode, int physical, int tile_low, int tc_chain, const qlb_gate_instr* prog,
+                           uint64_t count, const qlb_pool_view* pool, char* out, uint64_t cap, uint64_t* needed) {
     return guarded([&] {
         if (count && !prog) fail(QLB_ERR_INVALID_ARG, "program is null");
         if (n > 34) fail(QLB_ERR_INVALID_ARG, "at most 34 qubits");
         if (mode < QLB_MODE_PLAIN || mode > QLB_MODE_TILED_TC) fail(QLB_ERR_INVALID_ARG, "unknown execution mode");
         for (uint64_t i = 0; i < count; ++i) validate_instr(prog[i], n, pool);
-        const std::string js = describe_plan_json(PlanConfig{n, mode, physical, 10.0}, prog, count, pool);
+        const std::string js =
+            describe_plan_json(PlanConfig{n, mode, physical, 10.0, tc_chain != 0, tile_low}, prog, count, pool);
         if (needed) *needed = js.size() + 1;
         if (out && cap) {
             const size_t m = std::min<size_t>(cap - 1, js.size());
@@ -685,6 +691,10 @@ int qlb_engine_set_option(qlb_engine_t e, int key, int64_t value) {
             e->tc_min_cost = static_cast<double>(value) / 100.0;
         } else if (key == QLB_OPT_TC_CHAIN) {
             e->tc_chain = value != 0;
+        } else if (key == QLB_OPT_TILE_LOW) {
+            if (value < kTileLow || value > kTileLowMax)
+                fail(QLB_ERR_INVALID_ARG, "QLB_OPT_TILE_LOW must be in 3..6");
+            e->tile_low = static_cast<int>(value);
         } else {
             fail(QLB_ERR_INVALID_ARG, "unknown engine option");
         }

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/qlassical_b200.h"
+#include "tile.h"
 
 struct qlb_state {
     float2* d = nullptr;   // 2^n complex64 amplitudes (cudaMalloc, 256-B aligned)
@@ -69,6 +70,7 @@ struct qlb_engine {
     int physical_global_swap = 0;   // execute GLOBAL_SWAP as a data permutation
     double tc_min_cost = 10.0;      // TILED_TC: smallest fused-run cost sent to the tensor cores
     int tc_chain = 1;               // TILED_TC: chain kernel for passes of tensor-core ops only
+    int tile_low = qlb::kTileLow;   // tiled modes: memory qubits 0..tile_low-1 in every tile
     qlb::DeviceBuffer red_partial, red_out, staging, err_flag, exec_plan;   // exec_plan: execute()'s plan image   // err_flag: device int set by bounded waits
     qlb::PinnedBuffer host_pinned, host_prog;
     qlb_exec_stats stats{};

@@ -46,6 +46,7 @@ struct PlanConfig {
     int physical_global_swap;
     double tc_min_cost = 10.0;   // TILED_TC: smallest fused-run cost sent to the tensor cores
     int tc_chain = 1;            // TILED_TC: passes of tensor-core ops only run on the chain kernel
+    int tile_low = kTileLow;     // memory qubits 0..tile_low-1 are in every tile (kTileLow..kTileLowMax)
 };
 // Host-only planning: the plan as JSON (steps, passes, phases, ops, matrices).
 std::string describe_plan_json(const PlanConfig& cfg, const qlb_gate_instr* prog, uint64_t count,

@@ -385,7 +385,8 @@ int qlb_server_create(qlb_server_t* out, const qlb_server_config* cfg) {
             L.meta_host.ensure(meta_bytes);
             L.err_dev.ensure(256);
             L.err_host.ensure(sizeof(int));
-            check_cuda(cudaMemset(L.err_dev.p, 0, sizeof(int)), "error flag");
+            check_cuda(cudaMemsetAsync(L.err_dev.p, 0, sizeof(int), L.stream), "error flag");
+            check_cuda(cudaStreamSynchronize(L.stream), "error flag");
         }
         check_cuda(configure_tile_kernel(), "tile kernel attributes");
         s->info.arena_bytes = bytes;

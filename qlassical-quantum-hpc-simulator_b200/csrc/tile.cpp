@@ -26,8 +26,6 @@ namespace qlb {
 
 namespace {
 
-constexpr uint64_t kLowMask = (uint64_t{1} << kTileLow) - 1;  // memory qubits in every tile
-
 struct Term {            // diagonal factor exp(i*angle) on amplitudes whose qubits a (and b) are 1
     int a, b;            // -1 = absent (a < 0: a global phase)
     double angle;        // radians
@@ -301,7 +299,12 @@ void fill_reg(std::vector<int>& reg, bool edge) {
 
 class Planner {
 public:
-    Planner(const PlanConfig& cfg, const qlb_pool_view* pool) : e_(cfg), pool_(pool), n_(cfg.n) {}
+    Planner(const PlanConfig& cfg, const qlb_pool_view* pool)
+        : e_(cfg), pool_(pool), n_(cfg.n), low_mask_((uint64_t{1} << cfg.tile_low) - 1) {
+        if (cfg.tile_low < kTileLow || cfg.tile_low > kTileLowMax)
+            fail(QLB_ERR_INVALID_ARG, "tile_low must be in " + std::to_string(kTileLow) + ".." +
+                                          std::to_string(kTileLowMax));
+    }
 
     std::vector<MI> mi;
     TileProgram prog;
@@ -415,15 +418,15 @@ public:
             uint64_t blocked = 0;
             for (size_t i = 0; i < window && seeds.size() < kSeeds; ++i) {
                 const MI& m = mi[pending[i]];
-                if (!(m.touched & blocked) && (m.targets & ~kLowMask)) seeds.push_back(static_cast<int>(i));
+                if (!(m.touched & blocked) && (m.targets & ~low_mask_)) seeds.push_back(static_cast<int>(i));
                 blocked |= m.touched;
             }
         }
-        uint64_t best_T = kLowMask;
+        uint64_t best_T = low_mask_;
         long best_score = -1;
         for (int seed : seeds) {
             std::vector<char> in(pending.size(), 0);
-            uint64_t T = kLowMask;
+            uint64_t T = low_mask_;
             if (seed >= 0) {
                 in[static_cast<size_t>(seed)] = 1;
                 T |= mi[pending[static_cast<size_t>(seed)]].targets;
@@ -519,6 +522,7 @@ private:
     PlanConfig e_;
     const qlb_pool_view* pool_;
     uint32_t n_;
+    uint64_t low_mask_;   // memory qubits in every tile
 
     void build_pass(uint64_t T, const std::vector<uint32_t>& ops, bool final_pass) {
         // fill the tile with the lowest unused memory qubits
@@ -1409,7 +1413,7 @@ HostPlan plan_host(const PlanConfig& cfg, const qlb_gate_instr* prog, uint64_t c
 
 qlb_plan* compile_plan(qlb_engine& e, const qlb_gate_instr* prog, uint64_t count, const qlb_pool_view* pool,
                        DeviceBuffer* image) {
-    Planner pl(PlanConfig{e.sv.n, e.mode, e.physical_global_swap, e.tc_min_cost, e.tc_chain}, pool);
+    Planner pl(PlanConfig{e.sv.n, e.mode, e.physical_global_swap, e.tc_min_cost, e.tc_chain, e.tile_low}, pool);
     pl.plan(prog, count);
     TileProgram& tp = pl.prog;
     auto* p = new qlb_plan();

@@ -748,8 +748,8 @@ __device__ __forceinline__ uint32_t find_work(const TileWork* __restrict__ work,
 // a different pass.
 template <int LEVEL>
 __global__ void __launch_bounds__(NT, 1)
-k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work, uint64_t ntiles, int features,
-            int* __restrict__ err) {
+k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work, const uint32_t* __restrict__ tile_entry,
+            uint64_t ntiles, int features, int* __restrict__ err) {
     const int has_tc = features & kPassTensorCores;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     float2* bufs = reinterpret_cast<float2*>(smem_raw);
@@ -778,7 +778,10 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
     TcCtx tc{has_tc ? *tmem_holder : 0u, &bar[2], sb, 0u};
     bool failed = false;
 
-    auto entry = [&](uint64_t t) -> TileWork { return n_work ? work[find_work(work, n_work, t)] : single; };
+    auto entry = [&](uint64_t t) -> TileWork {
+        if (!n_work) return single;
+        return work[tile_entry ? __ldg(tile_entry + t) : find_work(work, n_work, t)];
+    };
 
     // Stage the entry's pass: its descriptor, phases and (if they fit) ops.
     // Phase op ranges index the program's op array; the shared copy is rebased.
@@ -821,7 +824,10 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
     // staged in the transpose buffer and written back by bulk stores, which
     // drain while the CTA goes on; the next write into that buffer first
     // waits until the stores have read it.
+    // The CTA's tiles stride across the grid, over a work list too: tiles of
+    // unequal cost (entries of different passes) spread evenly over the CTAs.
     uint64_t tile = blockIdx.x;
+    const uint64_t stride = gridDim.x, end = ntiles;
     float2* xbuf = bufs + 2 * static_cast<size_t>(TILE);
     auto issue_load = [&](uint64_t t, uint32_t slot) {
         const TileWork wl = entry(t);
@@ -831,8 +837,8 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
         issue_tile_load(bufs + static_cast<size_t>(slot) * TILE, wl.state, same ? *spass : wl.passes[wl.pass],
                         t - wl.tile_begin, &bar[slot]);
     };
-    if (tile < ntiles) issue_load(tile, 0);
-    if (tile + gridDim.x < ntiles) issue_load(tile + gridDim.x, 1);
+    if (tile < end) issue_load(tile, 0);
+    if (tile + stride < end) issue_load(tile + stride, 1);
     bool store_pending = false;      // uniform: a bulk store may still be reading xbuf
     auto xbuf_free = [&]() {
         if (store_pending) {
@@ -842,7 +848,7 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
         }
     };
     uint32_t it = 0;
-    for (; tile < ntiles; tile += gridDim.x, ++it) {
+    for (; tile < end; tile += stride, ++it) {
         const TileWork w = entry(tile);
         if (w.pass != staged || w.passes != staged_prog) {   // uniform: every thread reads the same entry
             __syncthreads();
@@ -852,11 +858,11 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
         const TilePass& P = *spass;
         const uint32_t b = it & 1u;
         float2* cur = bufs + static_cast<size_t>(b) * TILE;
-        const uint64_t next = tile + gridDim.x;
+        const uint64_t next = tile + stride;
         const bool ok = mbar_wait_bounded(&bar[b], (it >> 1) & 1u);
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) atomicExch(err, 1);
-            if (next < ntiles) mbar_wait_bounded(&bar[b ^ 1u], ((it + 1) >> 1) & 1u);
+            if (next < end) mbar_wait_bounded(&bar[b ^ 1u], ((it + 1) >> 1) & 1u);
             failed = true;
             break;
         }
@@ -896,7 +902,7 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
         }
         if (!good) {     // a tensor-core wait gave up (every thread agrees)
             if (threadIdx.x == 0) atomicExch(err, 2);
-            if (next < ntiles) mbar_wait_bounded(&bar[b ^ 1u], ((it + 1) >> 1) & 1u);
+            if (next < end) mbar_wait_bounded(&bar[b ^ 1u], ((it + 1) >> 1) & 1u);
             failed = true;
             break;
         }
@@ -910,13 +916,13 @@ k_tile_pass(TileWork single, const TileWork* __restrict__ work, uint32_t n_work,
             __syncthreads();
             issue_tile_store(xbuf, state, P, tile - w.tile_begin);
             store_pending = true;
-            if (next + gridDim.x < ntiles) issue_load(next + gridDim.x, b);
+            if (next + stride < end) issue_load(next + stride, b);
         } else {
             // Short runs: store from registers (the last phase's lanes are
             // tile positions 0..4, so a warp writes runs of >= 64 contiguous bytes).
             __syncthreads();             // every thread is done with cur
             fence_proxy_async();         // ... before the async-proxy writes of the next load
-            if (next + gridDim.x < ntiles) issue_load(next + gridDim.x, b);
+            if (next + stride < end) issue_load(next + stride, b);
             const TilePhase& last = phases[nph - 1];
             uint64_t ge[kRegQubits];
 #pragma unroll
@@ -983,20 +989,20 @@ cudaError_t configure_tile_kernel() {
 }
 
 namespace {
-void launch_tile_kernel(unsigned grid, const TileWork& single, const TileWork* work, uint32_t n_work, uint64_t ntiles,
-                        int features, int* err, cudaStream_t s) {
+void launch_tile_kernel(unsigned grid, const TileWork& single, const TileWork* work, uint32_t n_work,
+                        const uint32_t* tile_entry, uint64_t ntiles, int features, int* err, cudaStream_t s) {
     switch (tile_body(features)) {
     case kBodyWide:
-        k_tile_pass<kLevelWide><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
+        k_tile_pass<kLevelWide><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, tile_entry, ntiles, features, err);
         break;
     case kBodyTc:
-        k_tile_pass<kLevelTc><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
+        k_tile_pass<kLevelTc><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, tile_entry, ntiles, features, err);
         break;
     case kBodySwaps:
-        k_tile_pass<kLevelSwaps><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
+        k_tile_pass<kLevelSwaps><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, tile_entry, ntiles, features, err);
         break;
     default:
-        k_tile_pass<kLevelNarrow><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, ntiles, features, err);
+        k_tile_pass<kLevelNarrow><<<grid, NT, kSmemTotal, s>>>(single, work, n_work, tile_entry, ntiles, features, err);
         break;
     }
 }
@@ -1011,12 +1017,12 @@ cudaError_t launch_tile_pass(float2* state, uint32_t n, const TilePass* d_passes
     uint64_t grid = static_cast<uint64_t>(sm_count());
     if (grid > tiles) grid = tiles;
     const TileWork single{state, 0, d_passes, d_phases, d_ops, d_mats, pass_index, 0};
-    launch_tile_kernel(static_cast<unsigned>(grid), single, nullptr, 0, tiles, features, err, s);
+    launch_tile_kernel(static_cast<unsigned>(grid), single, nullptr, 0, nullptr, tiles, features, err, s);
     return cudaGetLastError();
 }
 
 cudaError_t launch_tile_work(const TileWork* d_work, uint32_t n_work, uint64_t total_tiles, int features, int* err,
-                             cudaStream_t s, uint32_t max_ctas) {
+                             cudaStream_t s, uint32_t max_ctas, const uint32_t* d_tile_entry) {
     if (n_work == 0 || total_tiles == 0) return cudaSuccess;
     cudaError_t e = configure_tile_kernel();
     if (e != cudaSuccess) return e;
@@ -1024,7 +1030,7 @@ cudaError_t launch_tile_work(const TileWork* d_work, uint32_t n_work, uint64_t t
     if (max_ctas && grid > max_ctas) grid = max_ctas;
     if (grid > total_tiles) grid = total_tiles;
     const TileWork none{nullptr, 0, nullptr, nullptr, nullptr, nullptr, 0, 0};
-    launch_tile_kernel(static_cast<unsigned>(grid), none, d_work, n_work, total_tiles, features, err, s);
+    launch_tile_kernel(static_cast<unsigned>(grid), none, d_work, n_work, d_tile_entry, total_tiles, features, err, s);
     return cudaGetLastError();
 }
 

@@ -40,6 +40,7 @@ constexpr int kThreadQubits = 8;         // 256 threads
 constexpr int kTileThreads = 1 << kThreadQubits;
 constexpr int kLaneLow = 5;              // lanes of the first and last phase: tile positions 0..4
 constexpr int kTileLow = 3;              // memory qubits 0..kTileLow-1 are in every tile
+constexpr int kTileLowMax = 6;           // a planner may keep up to this many (runs of 2^k amplitudes)
 constexpr uint32_t kMaxSmemOps = 160;    // ops of one pass cached in shared memory
 constexpr uint32_t kMaxSmemPhases = 24;
 constexpr uint32_t kDiagStageWords = 1024; // 16-byte words of DIAG data staged in shared memory (16 KB)
@@ -223,9 +224,11 @@ cudaError_t launch_wait_selftest(uint64_t limit_ns, int* err, cudaStream_t s);
 // capturing a launch into a CUDA graph).
 cudaError_t configure_tile_kernel();
 // One launch over a work list in device memory (batched and served states);
-// `max_ctas` caps the grid (0: one CTA per SM).
+// `max_ctas` caps the grid (0: one CTA per SM).  `d_tile_entry` (optional):
+// the work-list index of every tile of the launch, which replaces the
+// kernel's binary search over the entries' tile_begin.
 cudaError_t launch_tile_work(const TileWork* d_work, uint32_t n_work, uint64_t total_tiles, int features, int* err,
-                             cudaStream_t s, uint32_t max_ctas = 0);
+                             cudaStream_t s, uint32_t max_ctas = 0, const uint32_t* d_tile_entry = nullptr);
 
 // Host-side helpers shared between engine.cpp and tile.cpp.
 struct Layout {

@@ -102,8 +102,10 @@ def set_device(device: int) -> None:
 
 
 def describe_plan(program, num_qubits: int, mode: str = "tiled", pool: Optional[UnitaryPool] = None,
-                  physical_global_swap: bool = False) -> dict:
-    """EXPLAIN: the engine's plan for `program` (host-only, no GPU needed)."""
+                  physical_global_swap: bool = False, tile_low: int = 3, tc_chain: bool = True) -> dict:
+    """EXPLAIN: the engine's plan for `program` (host-only, no GPU needed).
+    tile_low and tc_chain are the planner options QLB_OPT_TILE_LOW and
+    QLB_OPT_TC_CHAIN."""
     import json
     if isinstance(program, IRModule):
         pool = program.unitaries()
@@ -112,17 +114,18 @@ def describe_plan(program, num_qubits: int, mode: str = "tiled", pool: Optional[
     pool = pool if pool is not None else UnitaryPool()
     pv, keep = pool.view()
     L = lib()
-    fn = L.qlb_describe_plan
-    fn.argtypes = [ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
-                   ctypes.POINTER(_lib.PoolView), ctypes.c_char_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]
+    fn = L.qlb_describe_plan_opts
+    fn.argtypes = [ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                   ctypes.c_uint64, ctypes.POINTER(_lib.PoolView), ctypes.c_char_p, ctypes.c_uint64,
+                   ctypes.POINTER(ctypes.c_uint64)]
     fn.restype = ctypes.c_int
     m = MODES[mode] if isinstance(mode, str) else int(mode)
+    opts = (num_qubits, m, int(physical_global_swap), int(tile_low), int(bool(tc_chain)), _lib.ptr(prog), prog.size,
+            ctypes.byref(pv))
     need = ctypes.c_uint64()
-    _lib.check(fn(num_qubits, m, int(physical_global_swap), _lib.ptr(prog), prog.size, ctypes.byref(pv), None, 0,
-                  ctypes.byref(need)))
+    _lib.check(fn(*opts, None, 0, ctypes.byref(need)))
     buf = ctypes.create_string_buffer(need.value)
-    _lib.check(fn(num_qubits, m, int(physical_global_swap), _lib.ptr(prog), prog.size, ctypes.byref(pv), buf,
-                  need.value, ctypes.byref(need)))
+    _lib.check(fn(*opts, buf, need.value, ctypes.byref(need)))
     del keep
     return json.loads(buf.value.decode())
 

@@ -55,13 +55,8 @@ class TranspilerConfig:
         self.cost_model_type = CostModelType.CUSTOM
 
 
-_COST_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
-                            ctypes.POINTER(ctypes.c_uint16), ctypes.POINTER(ctypes.c_uint16), ctypes.c_uint32,
-                            ctypes.POINTER(ctypes.c_uint16), ctypes.POINTER(ctypes.c_uint16))
-
-
-class _TranspileConfigC(ctypes.Structure):
-    _fields_ = _lib.TranspileConfig._fields_ + [("custom_cost_model", _COST_FN), ("custom_cost_model_ctx", ctypes.c_void_p)]
+_COST_FN = _lib.COST_MODEL_FN
+_TranspileConfigC = _lib.TranspileConfig
 
 
 def gpu_safe_qubit_limit() -> int:

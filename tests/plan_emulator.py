@@ -166,14 +166,14 @@ def apply_diag(st, n, mq, op, words, tq):
     st *= fac
 
 
-_tc_cache = {}
-
-
 def decode_tc_flat(plan, data, flags=None):
     """The split-precision unitary of a tensor-core op from its B image: row
     n = 2r + ro, column k = 2 kappa(c) + ri, kappa placing bit j of c at bit
-    (flags >> 3j) & 7 (identity when flags is None)."""
-    key = (id(plan), data, flags)
+    (flags >> 3j) & 7 (identity when flags is None).  Decoded matrices are
+    cached in the plan dict itself (an id()-keyed global cache would hand a
+    freed plan's matrices to a new plan that reuses its id)."""
+    _tc_cache = plan.setdefault("_tc_cache", {})
+    key = (data, flags)
     if key not in _tc_cache:
         flat = np.array(plan["mats"], dtype=np.uint32)    # raw words, 2 per float2 slot
         raw = flat[2 * data:2 * data + 4096].tobytes()

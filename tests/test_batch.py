@@ -104,3 +104,46 @@ def test_batch_edge_cases():
         Batch([qc.release()], "tiled")
     with pytest.raises(ValueError):
         Batch([], "tiled")
+
+
+@pytest.mark.gpu
+def test_autotuner_search_is_recorded_and_results_hold():
+    """mode "auto": one tune entry per size class, every candidate timed on
+    its sample, one mode for the batch and per class the fastest fixed-low
+    count in it, and every circuit's <Z> still matches the oracle whichever
+    configuration planned it."""
+    mods = circuits.hea_batch(40, seed=13, n_min=10, n_max=17, d_min=4, d_max=10)
+    b = Batch(mods, "auto")
+    b.run()
+    b.synchronize()
+    st = b.stats()
+    sizes = sorted({max(13, m.num_qubits) for m in mods})
+    assert [t["num_qubits"] for t in st["tune"]] == sizes
+    assert sum(t["circuits"] for t in st["tune"]) == len(mods)
+    assert len({t["best"]["mode"] for t in st["tune"]}) == 1
+    for t in st["tune"]:
+        assert 1 <= t["sample"] <= t["circuits"]
+        assert all(x > 0 for x in t["ms"]), t
+        base = 0 if t["best"]["mode"] == "tiled" else 3
+        best = min(range(base, base + 3), key=lambda k: t["ms"][k])
+        assert t["best"] == q._lib.batch_tune_candidate(best)
+    assert st["tune_seconds"] > 0 and st["autotune_ms"][0] <= st["autotune_ms"][1] + 1e-9
+    ez = b.expect_z()
+    for i, m in enumerate(mods):
+        want, _ = _oracle_ez(m)
+        assert np.max(np.abs(ez[i] - want)) < 5e-5, (i, m.num_qubits)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["tiled", "tiled_tc"])
+@pytest.mark.parametrize("tile_low", [4, 5, 6])
+def test_engine_tile_low_option(mode, tile_low):
+    """QLB_OPT_TILE_LOW on the single-circuit engine: same state as the oracle."""
+    m = circuits.hea(17, 10, 3)
+    e = q.CUDAEngine(17, mode=mode)
+    e.set_option(q._lib.OPT_TILE_LOW, tile_low)
+    e.execute(m)
+    st, _ = oracle.run_oracle(m)
+    assert oracle.max_abs_diff(st, e.state()) < 2e-5
+    with pytest.raises(ValueError):
+        e.set_option(q._lib.OPT_TILE_LOW, 7)

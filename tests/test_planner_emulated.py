@@ -14,8 +14,8 @@ import zoo
 TOL = {"tiled": 2e-5, "tiled_tc": 5e-5}
 
 
-def check(module, mode, init=None, physical=False):
-    plan = describe_plan(module, module.num_qubits, mode, physical_global_swap=physical)
+def check(module, mode, init=None, physical=False, **opts):
+    plan = describe_plan(module, module.num_qubits, mode, physical_global_swap=physical, **opts)
     want, _ = oracle.run_oracle(module, init=init)
     got = emulate(plan, init=init)
     d = oracle.max_abs_diff(want, got)
@@ -29,6 +29,27 @@ def check(module, mode, init=None, physical=False):
 def test_zoo_all_types(n, mode):
     m = zoo.random_circuit(n, 250, seed=n, types=zoo.REF_TYPES + zoo.EXT_TYPES, max_dense=5)
     check(m, mode)
+
+
+@pytest.mark.parametrize("mode", ["tiled", "tiled_tc"])
+@pytest.mark.parametrize("tile_low", [4, 5, 6])
+def test_fixed_low_tile_qubits(tile_low, mode):
+    """QLB_OPT_TILE_LOW: memory qubits 0..tile_low-1 are in every tile of
+    every pass (runs of 2^tile_low amplitudes), with the same results."""
+    m = zoo.random_circuit(16, 200, seed=40 + tile_low, types=zoo.REF_TYPES + zoo.EXT_TYPES, max_dense=5)
+    plan = check(m, mode, tile_low=tile_low, tc_chain=False)
+    for p in plan["passes"]:
+        assert p["tile_pos"][:tile_low] == list(range(tile_low))
+        assert p["n_low"] >= tile_low
+    h = circuits.hea(18, 12, 5)
+    check(h, mode, tile_low=tile_low, tc_chain=False)
+
+
+def test_tile_low_out_of_range_is_rejected():
+    m = circuits.hea(14, 2, 1)
+    for bad in (2, 7):
+        with pytest.raises(ValueError):
+            describe_plan(m, 14, "tiled", tile_low=bad)
 
 
 @pytest.mark.parametrize("mode", ["tiled", "tiled_tc"])
