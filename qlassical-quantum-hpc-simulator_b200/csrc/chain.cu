@@ -6,7 +6,7 @@
 // embedding, hi/lo; FP32 accumulate in tensor memory; the operand layouts
 // are the general tile kernel's, tile.cu).  Between two ops the tile never
 // visits the register file longer than one conversion: tensor memory ->
-// registers (D1 + D2) -> bf16 hi/lo -> the next op's A operand in shared
+// registers (FP32) -> bf16 hi/lo -> the next op's A operand in shared
 // memory, scattered by the planner's per-bit XOR offsets.
 //
 // Where the general kernel runs one tile at a time and waits for every
@@ -61,7 +61,7 @@ constexpr size_t kSmemChain = kOffBar + 10 * 8 + 8 + 2 * 16;
 static_assert(sizeof(TilePass) % 8 == 0 && sizeof(TilePhase) % 4 == 0, "descriptor staging");
 static_assert(kSmemChain <= 227 * 1024, "shared memory per CTA");
 constexpr uint32_t kBPerThread = kTcBBytes / (16u * kCompute);   // 4 x 16 B of B per thread
-constexpr uint32_t kTmemCols = 512;               // two slots x (2 M-blocks x (D1 | D2))
+constexpr uint32_t kTmemCols = 512;               // two slots x 2 M-blocks x 128 columns (D: the first 64)
 
 __device__ __forceinline__ uint64_t tile_base(const TilePass& P, uint64_t tile) {
     uint64_t base = 0;
@@ -102,35 +102,65 @@ __device__ __forceinline__ bool compute_any(bool x) {
     return r != 0;
 }
 
-// Issues the 16 MMAs of one op on A at `a` (hi; lo 32 KB above), B at `b`,
-// D at tensor-memory column `d`: per M-block of 128 rows, A_hi x [B_hi |
-// B_lo] (N = 128) into D1 | D2, then A_lo x B_hi (N = 64) added into D1.
+// Issues the 24 MMAs of one op on A at `a` (hi; lo 32 KB above), B at `b`
+// (B_hi; B_lo 8 KB above: N rows 64..127 of the staged image), D at
+// tensor-memory column `d`: per M-block of 128 rows and K step, A_hi x B_hi,
+// A_hi x B_lo and A_lo x B_hi (N = 64), all accumulated into one D, so the
+// read-back is one FP32 value per word.  (Issuing A_hi x [B_hi | B_lo] as
+// one N = 128 MMA takes 16 MMAs but leaves two partial sums, D1 | D2, for
+// the compute threads to load and add: twice the tensor-memory loads.)
 __device__ __forceinline__ void issue_mmas(uint32_t a, uint32_t b, uint32_t d, uint64_t* bar) {
     tc_fence_after();   // after the wait that saw A and B written (and the previous D read)
 #pragma unroll
     for (uint32_t mb = 0; mb < 2; ++mb) {
         const uint32_t dm = d + mb * 128u;
 #pragma unroll
-        for (uint32_t s = 0; s < 4; ++s)
-            tc_mma(dm, umma_desc_a(a + mb * 16384u + s * 32u), umma_desc_b(b + s * 256u), kTcIdesc128, s > 0 ? 1u : 0u);
-#pragma unroll
-        for (uint32_t s = 0; s < 4; ++s)
+        for (uint32_t s = 0; s < 4; ++s) {
+            const uint64_t ahi = umma_desc_a(a + mb * 16384u + s * 32u);
+            tc_mma(dm, ahi, umma_desc_b(b + s * 256u), kTcIdesc64, s > 0 ? 1u : 0u);
+            tc_mma(dm, ahi, umma_desc_b(b + 8192u + s * 256u), kTcIdesc64, 1u);
             tc_mma(dm, umma_desc_a(a + 32768u + mb * 16384u + s * 32u), umma_desc_b(b + s * 256u), kTcIdesc64, 1u);
+        }
     }
     tc_commit(bar);
 }
 
-// Reads 8 amplitudes (register indices 8 q .. 8 q + 7) of this thread's D
-// row: D1 + D2, columns 16 q .. 16 q + 15 of each.
-__device__ __forceinline__ void read_quarter(uint32_t row, uint32_t q, float2 (&a)[8]) {
-    uint32_t r1[16], r2[16];
-    tc_ld_16(row + q * 16u, r1);
-    tc_ld_16(row + 64u + q * 16u, r2);
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+// tcgen05.wait::ld with the awaited registers as operands, so that no use
+// of them is scheduled above the wait.
+__device__ __forceinline__ void tmem_wait(uint32_t (&r)[16]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15])
+                 :
+                 : "memory");
+}
+
+// This thread's D row (32 amplitudes, columns 0..63 from `col`) in four
+// quarters of 8 amplitudes (register indices 8 h .. 8 h + 7), handed to
+// use(a, h).  The next quarter's tensor-memory load is in flight while the
+// current one is used.
+template <typename F>
+__device__ __forceinline__ void read_back(uint32_t col, F&& use) {
+    uint32_t ra[16], rb[16];
+    auto hand = [&](const uint32_t (&r)[16], uint32_t h) {
+        float2 a[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c)
-        a[c] = make_float2(__uint_as_float(r1[2 * c]) + __uint_as_float(r2[2 * c]),
-                           __uint_as_float(r1[2 * c + 1]) + __uint_as_float(r2[2 * c + 1]));
+        for (int c = 0; c < 8; ++c) a[c] = make_float2(__uint_as_float(r[2 * c]), __uint_as_float(r[2 * c + 1]));
+        use(a, h);
+    };
+    tc_ld_16(col, ra);
+    tmem_wait(ra);
+    tc_ld_16(col + 16u, rb);
+    hand(ra, 0u);
+    tmem_wait(rb);
+    tc_ld_16(col + 32u, ra);
+    hand(rb, 1u);
+    tmem_wait(ra);
+    tc_ld_16(col + 48u, rb);
+    hand(ra, 2u);
+    tmem_wait(rb);
+    hand(rb, 3u);
 }
 
 // Scatters amplitudes with register indices base_r .. base_r + N - 1 into
@@ -426,10 +456,7 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                             le[i] ^= fold4(le[i]);
                         }
                         float2* dst = reinterpret_cast<float2*>(buf);
-#pragma unroll
-                        for (uint32_t h = 0; h < 4; ++h) {
-                            float2 a[8];
-                            read_quarter(dcol + drow, h, a);
+                        read_back(dcol + drow, [&](const float2 (&a)[8], uint32_t h) {
 #pragma unroll
                             for (uint32_t c = 0; c < 8; ++c) {
                                 const uint32_t r = 8u * h + c;
@@ -439,7 +466,7 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                                     if ((r >> i) & 1u) l ^= le[i];
                                 dst[l] = a[c];
                             }
-                        }
+                        });
                         tc_fence_before();
                         __syncwarp();
                         if ((t & 31u) == 0) mbar_arrive(&staged[b]);   // for the whole warp
@@ -456,12 +483,8 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                         if ((t >> i) & 1u) thr ^= F.a_thr[i];
 #pragma unroll
                     for (int i = 0; i < kRegQubits; ++i) d[i] = F.a_reg[i];
-#pragma unroll
-                    for (uint32_t h = 0; h < 4; ++h) {
-                        float2 a[8];
-                        read_quarter(dcol + drow, h, a);
-                        scatter<8>(a, 8u * h, thr, d, buf);
-                    }
+                    read_back(dcol + drow,
+                              [&](const float2 (&a)[8], uint32_t h) { scatter<8>(a, 8u * h, thr, d, buf); });
                 }
                 // A and B go to the tensor core: the MMA warp issues once every
                 // compute thread has arrived
