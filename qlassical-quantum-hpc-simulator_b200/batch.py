@@ -94,7 +94,7 @@ class Batch:
             "tune_seconds": info.tune_seconds,
             "tune": [{"num_qubits": t.num_qubits, "circuits": t.circuits, "sample": t.sample,
                       "best": _lib.batch_tune_candidate(t.best),
-                      "ms": [round(float(x), 4) for x in t.ms]}
+                      "ms": [float(x) for x in t.ms]}
                      for t in info.tune[:info.tune_classes]],
         }
 

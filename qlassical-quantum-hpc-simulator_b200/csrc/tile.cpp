@@ -656,10 +656,12 @@ private:
         // missing one would be skipped by the kernel's dispatch).
         const int body = tile_body(pass_features_);
         for (uint32_t pi = P.phase_begin; pi < P.phase_end; ++pi)
-            for (uint32_t oi = prog.phases[pi].op_begin; oi < prog.phases[pi].op_end; ++oi)
+            for (uint32_t oi = prog.phases[pi].op_begin; oi < prog.phases[pi].op_end; ++oi) {
                 if (!tile_body_handles(body, prog.ops[oi].code))
                     fail(QLB_ERR_CUDA, "tile planner: op code " + std::to_string(prog.ops[oi].code) +
                                            " has no handler in kernel body " + std::to_string(body));
+                if (prog.ops[oi].code == OPC_KRON) ++oi;     // its continuation record
+            }
         PlanStep st{};
         st.kind = STEP_PASS;
         st.features = P.features;
@@ -1100,12 +1102,42 @@ private:
     std::vector<HostOp> rot_buf_;   // commuting 1-qubit rotations awaiting emission
     uint32_t rot_bits_ = 0;          // their register bits
 
+    // Four or five real rotations (on distinct register bits) become one
+    // TOP_KRON op: one dispatch for the run, identity on a missing bit.
+    static constexpr int kKronMin = 4;
     void flush_rotations() {
         std::stable_sort(rot_buf_.begin(), rot_buf_.end(),
                          [](const HostOp& a, const HostOp& b) { return a.kind < b.kind; });
-        for (const HostOp& h : rot_buf_) emit_cuda_op(h);
+        int real = 0;
+        for (const HostOp& h : rot_buf_) real += h.kind == TOP_U1R;
+        for (const HostOp& h : rot_buf_)
+            if (h.kind != TOP_U1R || real < kKronMin) emit_cuda_op(h);
+        if (real >= kKronMin) emit_kron();
         rot_buf_.clear();
         rot_bits_ = 0;
+    }
+    void emit_kron() {
+        float q[kRegQubits][4];
+        for (int j = 0; j < kRegQubits; ++j) {
+            q[j][0] = 1.f;
+            q[j][1] = 0.f;
+            q[j][2] = 0.f;
+            q[j][3] = 1.f;
+        }
+        for (const HostOp& h : rot_buf_)
+            if (h.kind == TOP_U1R)
+                for (int i = 0; i < 4; ++i) q[h.r0][i] = static_cast<float>(h.m[i].real());
+        TileOp op{}, cont{};
+        op.kind = TOP_KRON;
+        op.code = OPC_KRON;
+        std::memcpy(&op.m[0], q[0], 16);
+        std::memcpy(&op.m[2], q[1], 16);
+        cont.code = OPC_NOP;
+        std::memcpy(&cont.flags, q[2], 16);     // word 1: flags, n, ctrl_mem
+        std::memcpy(&cont.m[0], q[3], 16);
+        std::memcpy(&cont.m[2], q[4], 16);
+        prog.ops.push_back(op);
+        prog.ops.push_back(cont);
     }
 
     void flush_pending(const PhaseBuild& pb, const int* local_of, Acc* acc, bool global) {
@@ -1554,7 +1586,21 @@ std::string describe_plan_json(const PlanConfig& cfg, const qlb_gate_instr* prog
                     out += ",";
                     num(op.m[j].y);
                 }
-                out += "]}";
+                out += "]";
+                if (op.code == OPC_KRON && o + 1 < T.op_end) {   // the five factors, bit 0 first
+                    const TileOp& c = pl.prog.ops[o + 1];
+                    float q[20];
+                    std::memcpy(q, &op.m[0], 32);
+                    std::memcpy(q + 8, &c.flags, 16);
+                    std::memcpy(q + 12, &c.m[0], 32);
+                    out += ",\"kron\":[";
+                    for (int j = 0; j < 20; ++j) {
+                        if (j) out += ",";
+                        num(q[j]);
+                    }
+                    out += "]";
+                }
+                out += "}";
             }
             out += "]}";
         }

@@ -559,6 +559,16 @@ __device__ __forceinline__ void op_cphase(float2 (&v)[NR], uint32_t cm, float2 p
         if ((static_cast<uint32_t>(i) & cm) == cm) v[i] = cmul(v[i], p);
 }
 
+// One factor of a TOP_KRON op: the real 2x2 q = (m00, m01, m10, m11) on register bit RR.
+template <int RR>
+__device__ __forceinline__ void kron_bit(float2 (&v)[NR], uint4 q) {
+    const float2 m0 = make_float2(__uint_as_float(q.x), __uint_as_float(q.x));
+    const float2 m1 = make_float2(__uint_as_float(q.y), __uint_as_float(q.y));
+    const float2 m2 = make_float2(__uint_as_float(q.z), __uint_as_float(q.z));
+    const float2 m3 = make_float2(__uint_as_float(q.w), __uint_as_float(q.w));
+    for_pairs<RR>(v, [&](float2& x, float2& y) { u1r_pair2(x, y, m0, m1, m2, m3); });
+}
+
 // Kernel instantiations by code body: 1-qubit, controlled and diagonal ops
 // (kLevelNarrow); those plus register SWAPs (kLevelSwaps); uncontrolled
 // 1-qubit rotations, diagonal, SWAP, U2 and tensor-core ops (kLevelTc);
@@ -636,12 +646,22 @@ __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, co
         op_diag(v, tab, q1.x, q1.y & 0xFFFFu, q1.y >> 16, cm, M.gt);                                  \
         if (staged) __syncthreads();   /* the staging area is free again */                           \
     } break;
+#define QLB_KRON_CASE                                                                                 \
+    case OPC_KRON: {                                                                                  \
+        kron_bit<0>(v, rec[4 * oi + 2]);                                                              \
+        kron_bit<1>(v, rec[4 * oi + 3]);                                                              \
+        kron_bit<2>(v, rec[4 * oi + 5]);                                                              \
+        kron_bit<3>(v, rec[4 * oi + 6]);                                                              \
+        kron_bit<4>(v, rec[4 * oi + 7]);                                                              \
+        ++oi;                          /* the continuation record */                                  \
+    } break;
 #define QLB_COMMON_CASES                                                                              \
     QLB_U1R_CASE(0) QLB_U1R_CASE(1) QLB_U1R_CASE(2) QLB_U1R_CASE(3) QLB_U1R_CASE(4)                   \
     QLB_RX_CASE(0) QLB_RX_CASE(1) QLB_RX_CASE(2) QLB_RX_CASE(3) QLB_RX_CASE(4)                        \
     QLB_U1_CASE(0) QLB_U1_CASE(1) QLB_U1_CASE(2) QLB_U1_CASE(3) QLB_U1_CASE(4)                        \
     QLB_X_CASE(0) QLB_X_CASE(1) QLB_X_CASE(2) QLB_X_CASE(3) QLB_X_CASE(4)                             \
     QLB_DIAG_CASE                                                                                     \
+    QLB_KRON_CASE                                                                                     \
     case OPC_CPHASE:                                                                                  \
         op_cphase(v, cm, f2(rec[4 * oi + 2].x, rec[4 * oi + 2].y));                                  \
         break;
@@ -668,6 +688,7 @@ __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, co
                 QLB_RX_CASE(0) QLB_RX_CASE(1) QLB_RX_CASE(2) QLB_RX_CASE(3) QLB_RX_CASE(4)
                 QLB_U1_NC_CASE(0) QLB_U1_NC_CASE(1) QLB_U1_NC_CASE(2) QLB_U1_NC_CASE(3) QLB_U1_NC_CASE(4)
                 QLB_DIAG_CASE
+                QLB_KRON_CASE
                 QLB_PAIR_CASES(0, 1) QLB_PAIR_CASES(0, 2) QLB_PAIR_CASES(0, 3) QLB_PAIR_CASES(0, 4)
                 QLB_PAIR_CASES(1, 2) QLB_PAIR_CASES(1, 3) QLB_PAIR_CASES(1, 4)
                 QLB_PAIR_CASES(2, 3) QLB_PAIR_CASES(2, 4) QLB_PAIR_CASES(3, 4)
@@ -721,6 +742,7 @@ __device__ __forceinline__ bool run_ops(float2 (&v)[NR], const TilePhase& ph, co
     return true;
 }
 #undef QLB_COMMON_CASES
+#undef QLB_KRON_CASE
 #undef QLB_U1R_CASE
 #undef QLB_RX_CASE
 #undef QLB_U1_CASE

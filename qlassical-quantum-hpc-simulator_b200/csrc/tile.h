@@ -55,7 +55,8 @@ enum TileOpKind : uint8_t {
     TOP_RX = 7,       // [[c, -is], [-is, c]] on r0, c = m[0].x, s = m[0].y
     TOP_CPHASE = 8,   // amplitudes with ctrl_reg/ctrl_mem bits all set *= m[0]
     TOP_DENSE_TC = 9, // k = 5 on register bits 0..4 on the tensor cores
-    TOP_DIAG = 11     // a run of diagonal gates: one phase factor per amplitude (layout below)
+    TOP_DIAG = 11,    // a run of diagonal gates: one phase factor per amplitude (layout below)
+    TOP_KRON = 12     // a real 2x2 on each of register bits 0..4 (two records, layout below)
 };
 
 // Device dispatch codes: one handler per (kind, register bit / bit pair,
@@ -76,7 +77,8 @@ enum TileOpCode : uint16_t {
     OPC_DENSE_TC = 54,
     OPC_DIAG = 55,
     OPC_CPHASE = 56,
-    OPC_COUNT = 57
+    OPC_KRON = 57,
+    OPC_COUNT = 58
 };
 // (a, b), a < b < 5  ->  0..9
 __host__ __device__ constexpr uint32_t reg_pair_index(uint32_t a, uint32_t b) { return a * (9u - a) / 2u + (b - a - 1u); }
@@ -97,6 +99,9 @@ __host__ __device__ constexpr uint32_t reg_pair_index(uint32_t a, uint32_t b) { 
 //     m[0].x      (u32 bits) 0, or the data's length in 16-byte words when the kernel is to
 //                 stage it in shared memory first; the data starts on a 16-byte boundary
 //                 and is padded to whole words
+//   TOP_KRON: five real 2x2 matrices (m00, m01, m10, m11), one per register bit, in two
+//     records: bit 0 in words 2 of this record, bit 1 in its word 3, bits 2, 3, 4 in words
+//     1, 2, 3 of the next record (code OPC_NOP, never dispatched: the op's handler skips it)
 struct TileOp {
     uint16_t code;          // TileOpCode
     uint8_t kind, k;        // TileOpKind; DENSE: k
@@ -191,13 +196,15 @@ constexpr int tile_body(int features) {
 // Whether kernel body `body` has a handler for dispatch code `code` (the
 // planner checks every op of a pass against the body the pass will run).
 constexpr bool tile_body_handles(int body, uint32_t code) {
-    const bool common = (code >= OPC_U1 && code < OPC_SWAP) || code == OPC_DIAG || code == OPC_CPHASE;
+    const bool common =
+        (code >= OPC_U1 && code < OPC_SWAP) || code == OPC_DIAG || code == OPC_CPHASE || code == OPC_KRON;
     const bool swap = code >= OPC_SWAP && code < OPC_U2;
     const bool u2 = code >= OPC_U2 && code < OPC_DENSE3;
     switch (body) {
     case kBodyWide: return code >= OPC_U1 && code < OPC_COUNT;
     case kBodyTc:
-        return (code >= OPC_U1 && code < OPC_X) || code == OPC_DIAG || swap || u2 || code == OPC_DENSE_TC;
+        return (code >= OPC_U1 && code < OPC_X) || code == OPC_DIAG || code == OPC_KRON || swap || u2 ||
+               code == OPC_DENSE_TC;
     case kBodySwaps: return common || swap;
     default: return common;
     }

@@ -10,6 +10,7 @@ import numpy as np
 
 TOP_U1, TOP_X, TOP_SWAP, TOP_U2, TOP_DENSE, TOP_U1R, TOP_RX, TOP_CPHASE, TOP_DENSE_TC = range(1, 10)
 TOP_DIAG = 11
+TOP_KRON = 12          # five real 2x2 factors, one per register bit (plus a continuation record, kind 0)
 STEP_PASS, STEP_PLAIN, STEP_MEASURE, STEP_SWAP = range(4)
 PASS_CHAIN = 32
 
@@ -58,6 +59,13 @@ def emulate(plan, init=None):
                     m = np.array(op["m"]).reshape(4, 2)
                     mc = m[:, 0] + 1j * m[:, 1]
                     kd = op["kind"]
+                    if kd == 0:                   # a TOP_KRON op's continuation record
+                        continue
+                    if kd == TOP_KRON:
+                        q = np.array(op["kron"]).reshape(5, 2, 2)
+                        for j in range(5):
+                            apply_k(st, n, [mq[j]], q[j])
+                        continue
                     if kd == TOP_U1:
                         apply_k(st, n, [mq[op["r0"]]], mc.reshape(2, 2), cmask)
                     elif kd == TOP_U1R:
