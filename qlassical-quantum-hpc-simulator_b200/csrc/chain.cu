@@ -109,24 +109,17 @@ __device__ __forceinline__ bool compute_any(bool x) {
 // read-back is one FP32 value per word.  (Issuing A_hi x [B_hi | B_lo] as
 // one N = 128 MMA takes 16 MMAs but leaves two partial sums, D1 | D2, for
 // the compute threads to load and add: twice the tensor-memory loads.)
-// The descriptors' start-address field is (address >> 4) in bits 0..13:
-// every operand of an op lies below 256 KB of the shared window (with room
-// for the per-block reserve in front of the dynamic allocation), so the
-// descriptor of base + offset is the base's descriptor + (offset >> 4).
-static_assert(kOffB + 2 * kTcBBytes + 16 * 1024 <= 256 * 1024, "descriptor address field");
 __device__ __forceinline__ void issue_mmas(uint32_t a, uint32_t b, uint32_t d, uint64_t* bar) {
     tc_fence_after();   // after the wait that saw A and B written (and the previous D read)
-    const uint64_t da = umma_desc_a(a), db = umma_desc_b(b);
 #pragma unroll
     for (uint32_t mb = 0; mb < 2; ++mb) {
         const uint32_t dm = d + mb * 128u;
 #pragma unroll
         for (uint32_t s = 0; s < 4; ++s) {
-            const uint64_t ahi = da + ((mb * 16384u + s * 32u) >> 4);
-            const uint64_t bhi = db + ((s * 256u) >> 4);
-            tc_mma(dm, ahi, bhi, kTcIdesc64, s > 0 ? 1u : 0u);
-            tc_mma(dm, ahi, bhi + (8192u >> 4), kTcIdesc64, 1u);
-            tc_mma(dm, ahi + (32768u >> 4), bhi, kTcIdesc64, 1u);
+            const uint64_t ahi = umma_desc_a(a + mb * 16384u + s * 32u);
+            tc_mma(dm, ahi, umma_desc_b(b + s * 256u), kTcIdesc64, s > 0 ? 1u : 0u);
+            tc_mma(dm, ahi, umma_desc_b(b + 8192u + s * 256u), kTcIdesc64, 1u);
+            tc_mma(dm, umma_desc_a(a + 32768u + mb * 16384u + s * 32u), umma_desc_b(b + s * 256u), kTcIdesc64, 1u);
         }
     }
     tc_commit(bar);
