@@ -87,8 +87,8 @@ __device__ __forceinline__ bool producer_any(bool x) {
     return r != 0;
 }
 
-// Barrier 1 over the 256 compute threads (the load warp never joins it).
-__device__ __forceinline__ void compute_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+// Barrier 1 over the 256 compute threads (the producer and MMA warps never
+// join it), with an OR vote.
 __device__ __forceinline__ bool compute_any(bool x) {
     uint32_t r;
     asm volatile(
@@ -361,6 +361,7 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
         uint32_t uses[2] = {0u, 0u};
         bool pending[2] = {false, false};
         bool failed = false;
+        int bad = 0;             // the first wait of this thread that gave up (1: tile load, 2: MMA)
         const float2* __restrict__ mats = w.mats;
         for (;;) {
             bool active = false;
@@ -392,12 +393,7 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                 };
                 if (j == 0) {
                     // the loaded tile -> A of the first op
-                    const bool ok = mbar_wait_bounded(&full[b], (kk[s] / kBufs) & 1u);
-                    if (compute_any(!ok)) {
-                        failed = true;
-                        if (t == 0) atomicExch(err, 1);
-                        break;
-                    }
+                    if (!mbar_wait_bounded(&full[b], (kk[s] / kBufs) & 1u) && !bad) bad = 1;
                     copy_b();
                     const TilePhase& R = sph[0];
                     uint32_t tp = 0, e[kRegQubits];
@@ -416,7 +412,17 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                             if ((r >> i) & 1) l |= e[i];
                         v[r] = src[l];
                     }
-                    compute_sync();      // every thread has read the tile: the buffer becomes A
+                    // every thread has read the tile: the buffer becomes A.  The
+                    // same barrier is the vote on the waits that gave up since
+                    // the last one (a failed wait only leaves garbage in
+                    // bounds, so the steps in between ran on): all compute
+                    // threads leave together.
+                    if (compute_any(bad != 0)) {
+                        asm volatile("cp.async.wait_all;" ::: "memory");   // this step's B copy
+                        failed = true;
+                        if (bad) atomicExch(err, bad);
+                        break;
+                    }
                     if (first == 0) {
                         tc_write_a(v, buf, buf + 32768u);   // own row, identity K order
                     } else {
@@ -430,14 +436,11 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
                         scatter<32>(v, 0u, thr, d, buf);
                     }
                 } else {
-                    const bool ok = mbar_wait_bounded(&mmab[s], uses[s] & 1u);
+                    // no barrier here: a failed wait is voted on at the next
+                    // tile's first step
+                    if (!mbar_wait_bounded(&mmab[s], uses[s] & 1u) && !bad) bad = 2;
                     ++uses[s];
                     pending[s] = false;
-                    if (compute_any(!ok)) {
-                        failed = true;
-                        if (t == 0) atomicExch(err, 2);
-                        break;
-                    }
                     tc_fence_after();
                     if (j == m) {
                         // the last op's result, staged in its (now free) buffer:
