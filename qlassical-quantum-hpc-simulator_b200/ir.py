@@ -173,12 +173,14 @@ class IRModule:
         self.unitary_pool = unitary_pool if unitary_pool is not None else UnitaryPool()
 
     def program(self) -> np.ndarray:
-        if isinstance(self._gates, np.ndarray):
-            return self._gates
-        arr = np.zeros(len(self._gates), dtype=GATE_INSTR_DTYPE)
-        for i, g in enumerate(self._gates):
-            arr[i] = g
-        return arr
+        """The gate stream as one contiguous GateInstr array (the reference
+        keeps gate_stream contiguous).  Records appended one at a time are
+        packed on the first call and the packed array is kept until the next
+        append."""
+        if not isinstance(self._gates, np.ndarray):
+            self._gates = (np.array(self._gates, dtype=GATE_INSTR_DTYPE) if self._gates
+                           else np.zeros(0, dtype=GATE_INSTR_DTYPE))
+        return self._gates
 
     def set_program(self, arr: np.ndarray) -> None:
         self._gates = np.ascontiguousarray(arr, dtype=GATE_INSTR_DTYPE)
