@@ -24,9 +24,14 @@
 // MMA issue that waits for the tensor pipe to drain the other slot's MMAs
 // stalls nobody.  HBM traffic: 16 B per amplitude per pass.
 //
+// The compute warps meet at one CTA barrier per tile (before the loaded
+// tile becomes A); otherwise only the MMA dependency orders them, so a warp
+// that is ahead converts the other slot while the last one finishes.
+//
 // Every wait is bounded (2 s / 2^26 polls); on expiry the CTA raises *err,
 // waits (bounded) for its own MMAs and copies, frees its tensor memory and
-// returns.
+// returns.  A compute thread's wait that gives up is voted on at the next
+// per-tile barrier, so all compute threads leave together.
 #include "common.cuh"
 #include "tc_ptx.cuh"
 #include "tile.h"
