@@ -701,7 +701,10 @@ def serving_workload(q, args):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     mods = circuits.serving_requests(args.requests, seed=7)
     arrivals = circuits.poisson_arrivals(args.requests, args.rate, seed=11)
-    srv = Server()
+    # requests of >= 22 qubits are fused by the GPU middle end inside the
+    # server (blocks of up to 5 qubits) and run on the tensor cores; the
+    # smaller ones on FP32 tiles
+    srv = Server(fuse_from=22)
     # warm-up: a few small requests (kernel set-up, first launches)
     for m in circuits.serving_requests(4, seed=99, n_max=14):
         srv.result(srv.submit(m, shots=16, seed=1))
@@ -769,7 +772,9 @@ def serving_workload(q, args):
         "vs_baseline": None, "dtype": "c64 (fp32)", "data": "synthetic",
         "config": {"workload": f"{len(mods)} requests, Poisson arrivals at {args.rate}/s, random H/RX + CX-ladder "
                                f"circuits, n log-uniform in [12, 30], depth U{{10..40}}, 1024 shots + <Z_i>",
-                   "requests": len(mods), "rate_hz": args.rate, "lanes": "small (<22 qubits) / large, SM-partitioned"},
+                   "requests": len(mods), "rate_hz": args.rate, "lanes": "small (<22 qubits) / large, SM-partitioned",
+                   "plans": "< 22 qubits: FP32 tiles; >= 22: fused by the GPU middle end in the server (blocks of "
+                            "<= 5 qubits, no windowing), tensor-core tiles"},
         "p50_s": float(np.percentile(lat, 50)), "p99_s": p99, "mean_s": float(lat.mean()),
         "p50_small_s": float(np.percentile(lat[ns < 22], 50)),
         "p50_large_s": float(np.percentile(lat[ns >= 22], 50)) if np.any(ns >= 22) else None,

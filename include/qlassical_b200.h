@@ -395,6 +395,10 @@ typedef struct qlb_server_config {
     uint64_t memory_bytes;  /* device arena; 0 = 85% of the free HBM at creation */
     int      mode;          /* QLB_MODE_TILED (default) or QLB_MODE_TILED_TC */
     uint32_t max_active;    /* admitted requests at once; 0 = 4096 */
+    uint32_t fuse_from;     /* requests of at least this many qubits are first fused by the GPU
+                               middle end (qlb_transpile_gpu: blocks of up to 5 qubits, no
+                               windowing) and planned for the tensor cores; 0 = never */
+    uint32_t pad;
 } qlb_server_config;
 
 typedef struct qlb_server_info {

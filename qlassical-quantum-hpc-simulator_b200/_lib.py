@@ -131,7 +131,8 @@ class BatchInfo(ctypes.Structure):
 
 
 class ServerConfig(ctypes.Structure):
-    _fields_ = [("memory_bytes", ctypes.c_uint64), ("mode", ctypes.c_int), ("max_active", ctypes.c_uint32)]
+    _fields_ = [("memory_bytes", ctypes.c_uint64), ("mode", ctypes.c_int), ("max_active", ctypes.c_uint32),
+                ("fuse_from", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
 
 
 class ServerInfo(ctypes.Structure):

@@ -134,6 +134,7 @@ struct Lane {
 struct qlb_server {
     int device = 0;
     int mode = QLB_MODE_TILED;
+    uint32_t fuse_from = 0;            // requests of >= fuse_from qubits: fused, tensor-core plans
     uint32_t max_active = 4096;
     Arena arena;
     DeviceBuffer arena_mem;
@@ -361,6 +362,7 @@ int qlb_server_create(qlb_server_t* out, const qlb_server_config* cfg) {
         if (cfg) c = *cfg;
         if (c.mode != QLB_MODE_TILED && c.mode != QLB_MODE_TILED_TC) c.mode = QLB_MODE_TILED;
         s->mode = c.mode;
+        s->fuse_from = c.fuse_from;
         s->max_active = c.max_active ? std::min<uint32_t>(c.max_active, kMaxWork) : kMaxWork;
         check_cuda(cudaGetDevice(&s->device), "device");
         size_t free_b = 0, total_b = 0;
@@ -408,7 +410,29 @@ int qlb_server_submit(qlb_server_t s, const qlb_gate_instr* program, uint64_t co
         r->neff = std::max(num_qubits, kBatchMinQubits);
         r->shots = shots;
         r->seed = seed;
-        r->plan = plan_host(PlanConfig{r->neff, s->mode, 0, 10.0, 0}, program, count, pool ? pool : &empty);
+        if (s->fuse_from && num_qubits >= s->fuse_from) {
+            // the GPU middle end first: blocks of up to 5 qubits, no windowing
+            // (the plan then holds them as tensor-core ops)
+            qlb_transpile_config tc;
+            qlb_transpile_config_default(&tc);
+            tc.enable_hw_awareness = 0;
+            tc.max_fusion_qubits = 5;
+            qlb_module_t mod = nullptr;
+            if (qlb_transpile_gpu(program, count, pool ? pool : &empty, num_qubits, &tc, &mod) != QLB_OK)
+                fail(QLB_ERR_INVALID_ARG, std::string("request fusion: ") + qlb_last_error());
+            struct Guard {
+                qlb_module_t m;
+                ~Guard() { qlb_module_destroy(m); }
+            } guard{mod};
+            const qlb_gate_instr* fp = nullptr;
+            uint64_t fc = 0;
+            qlb_pool_view fpool{};
+            qlb_module_program(mod, &fp, &fc);
+            qlb_module_pool(mod, &fpool);
+            r->plan = plan_host(PlanConfig{r->neff, QLB_MODE_TILED_TC, 0, 10.0, 0}, fp, fc, &fpool);
+        } else {
+            r->plan = plan_host(PlanConfig{r->neff, s->mode, 0, 10.0, 0}, program, count, pool ? pool : &empty);
+        }
         for (const PlanStep& st : r->plan.steps)
             if (st.kind != STEP_PASS)
                 fail(QLB_ERR_INVALID_ARG, "served circuits may hold only gates (no MEASURE, no 6-qubit blocks)");

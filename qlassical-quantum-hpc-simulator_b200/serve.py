@@ -38,9 +38,12 @@ class Result:
 
 
 class Server:
-    def __init__(self, memory_bytes: int = 0, mode: str = "tiled", max_active: int = 0):
+    def __init__(self, memory_bytes: int = 0, mode: str = "tiled", max_active: int = 0, fuse_from: int = 0):
+        """fuse_from: requests of at least this many qubits are fused by the
+        GPU middle end (blocks of up to 5 qubits) and planned for the tensor
+        cores; the others run in `mode`.  0: no fusion."""
         cfg = _lib.ServerConfig(int(memory_bytes), _lib.MODE_TILED_TC if mode == "tiled_tc" else _lib.MODE_TILED,
-                                int(max_active))
+                                int(max_active), int(fuse_from), 0)
         h = ctypes.c_void_p()
         call("qlb_server_create", ctypes.byref(h), ctypes.byref(cfg))
         self._h = h

@@ -111,3 +111,23 @@ def test_serve_cancel_queued_and_admitted():
         c = circuits.random_h_rx_cx(14, 5, seed=4)
         st, _ = oracle.run_oracle(c)
         assert np.max(np.abs(srv.result(srv.submit(c, shots=0)).expect_z - circuits.expect_z_of(st, 14))) < 2e-5
+
+
+@pytest.mark.gpu
+def test_serve_fuses_large_requests():
+    """fuse_from: requests of at least that many qubits are fused by the GPU
+    middle end (blocks of up to 5 qubits) and planned for the tensor cores;
+    their <Z> still match the oracle, and the smaller requests are served
+    exactly as without fusion (bitwise)."""
+    from qlassical_b200.serve import Server
+    mods = circuits.serving_requests(10, seed=6, n_min=12, n_max=17, d_min=6, d_max=12)
+    assert any(m.num_qubits >= 15 for m in mods) and any(m.num_qubits < 15 for m in mods)
+    with Server(memory_bytes=1 << 30, fuse_from=15) as srv:
+        res = [srv.result(srv.submit(m, shots=256, seed=i)) for i, m in enumerate(mods)]
+    with Server(memory_bytes=1 << 30) as srv:
+        plain = [srv.result(srv.submit(m, shots=256, seed=i)) for i, m in enumerate(mods)]
+    for m, r, p in zip(mods, res, plain):
+        st, _ = oracle.run_oracle(m)
+        assert np.max(np.abs(r.expect_z - circuits.expect_z_of(st, m.num_qubits))) < 2e-5
+        if m.num_qubits < 15:
+            assert np.array_equal(r.expect_z, p.expect_z) and np.array_equal(r.samples, p.samples)
