@@ -365,6 +365,13 @@ typedef struct qlb_batch_info {
 int qlb_batch_create(qlb_batch_t* out, uint32_t count, const qlb_gate_instr* const* programs,
                      const uint64_t* counts, const qlb_pool_view* pools, const uint32_t* num_qubits,
                      int mode);
+/* The same, with every circuit first fused by the GPU middle end
+ * (qlb_transpile_gpu: blocks of up to fuse_qubits <= 5 qubits, no windowing)
+ * on host threads; 0 = no fusion (qlb_batch_create).  Fused blocks run best
+ * on the tensor cores (QLB_MODE_TILED_TC, or -1 to autotune). */
+int qlb_batch_create_ex(qlb_batch_t* out, uint32_t count, const qlb_gate_instr* const* programs,
+                        const uint64_t* counts, const qlb_pool_view* pools, const uint32_t* num_qubits,
+                        int mode, uint32_t fuse_qubits);
 /* Resets every state to |0...0>, runs all circuits and the FP64 <Z_i>
  * reductions: one graph launch on the batch's stream (asynchronous). */
 int qlb_batch_run(qlb_batch_t b);

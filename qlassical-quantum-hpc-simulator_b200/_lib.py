@@ -239,6 +239,7 @@ _SIGNATURES = {
     "qlb_check64_download": [_P, _P, _U64],
     "qlb_check64_destroy": [_P],
     "qlb_batch_create": [ctypes.POINTER(_P), _U32, _P, _P, _P, _P, _I],
+    "qlb_batch_create_ex": [ctypes.POINTER(_P), _U32, _P, _P, _P, _P, _I, _U32],
     "qlb_batch_run": [_P],
     "qlb_batch_synchronize": [_P],
     "qlb_batch_expect_z": [_P, _P, _U32],

@@ -29,7 +29,10 @@ _MODE_NAMES = {_lib.MODE_TILED: "tiled", _lib.MODE_TILED_TC: "tiled_tc", -1: "pe
 class Batch:
     """A planned batch; run() launches it, expect_z() reads the results."""
 
-    def __init__(self, modules: Sequence[IRModule], mode: str = "auto"):
+    def __init__(self, modules: Sequence[IRModule], mode: str = "auto", fuse: int = 0):
+        """fuse: blocks of up to this many qubits (<= 5) formed by the GPU
+        middle end in each circuit before planning (0: no fusion); fused
+        blocks run on the tensor cores."""
         if not modules:
             raise ValueError("empty batch")
         self._h = None
@@ -47,9 +50,9 @@ class Batch:
         pool_arr = (_lib.PoolView * n)(*pools)
         nq = (ctypes.c_uint32 * n)(*[int(mod.num_qubits) for mod in modules])
         h = ctypes.c_void_p()
-        call("qlb_batch_create", ctypes.byref(h), n, ctypes.cast(prog_ptrs, ctypes.c_void_p),
+        call("qlb_batch_create_ex", ctypes.byref(h), n, ctypes.cast(prog_ptrs, ctypes.c_void_p),
              ctypes.cast(counts, ctypes.c_void_p), ctypes.cast(pool_arr, ctypes.c_void_p),
-             ctypes.cast(nq, ctypes.c_void_p), m)
+             ctypes.cast(nq, ctypes.c_void_p), m, int(fuse))
         self._h = h
         self._n = n
         self._nq = [int(mod.num_qubits) for mod in modules]
@@ -104,9 +107,9 @@ class Batch:
         return s.value or 0
 
 
-def run_batch(modules: Sequence[IRModule], mode: str = "auto") -> list[np.ndarray]:
+def run_batch(modules: Sequence[IRModule], mode: str = "auto", fuse: int = 0) -> list[np.ndarray]:
     """Plans, runs and returns <Z_q> of every circuit."""
-    b = Batch(modules, mode)
+    b = Batch(modules, mode, fuse)
     b.run()
     b.synchronize()
     return b.expect_z()

@@ -422,7 +422,16 @@ extern "C" {
 
 int qlb_batch_create(qlb_batch_t* out, uint32_t count, const qlb_gate_instr* const* programs, const uint64_t* counts,
                      const qlb_pool_view* pools, const uint32_t* num_qubits, int mode) {
+    return qlb_batch_create_ex(out, count, programs, counts, pools, num_qubits, mode, 0);
+}
+
+int qlb_batch_create_ex(qlb_batch_t* out, uint32_t count, const qlb_gate_instr* const* programs_in,
+                        const uint64_t* counts_in, const qlb_pool_view* pools_in, const uint32_t* num_qubits,
+                        int mode, uint32_t fuse_qubits) {
     return guarded([&] {
+        const qlb_gate_instr* const* programs = programs_in;
+        const uint64_t* counts = counts_in;
+        const qlb_pool_view* pools = pools_in;
         need(out, "out");
         *out = nullptr;
         if (count == 0) fail(QLB_ERR_INVALID_ARG, "empty batch");
@@ -473,6 +482,55 @@ int qlb_batch_create(qlb_batch_t* out, uint32_t count, const qlb_gate_instr* con
         b->host_result.ensure(static_cast<size_t>(count) * kBatchStride * sizeof(double));
         b->host_err.ensure(sizeof(int));
         *static_cast<int*>(b->host_err.p) = 0;
+        // Fusion by the GPU middle end (blocks of up to fuse_qubits, no
+        // windowing), circuit by circuit on host threads; the batch is then
+        // planned from the fused programs (the counts above stay the logical
+        // gates').
+        struct Modules {
+            std::vector<qlb_module_t> m;
+            ~Modules() {
+                for (qlb_module_t x : m)
+                    if (x) qlb_module_destroy(x);
+            }
+        } fused;
+        std::vector<const qlb_gate_instr*> fprog;
+        std::vector<uint64_t> fcount;
+        std::vector<qlb_pool_view> fpool;
+        if (fuse_qubits) {
+            if (fuse_qubits > 5) fail(QLB_ERR_INVALID_ARG, "batched fusion takes blocks of at most 5 qubits");
+            fused.m.assign(count, nullptr);
+            fprog.assign(count, nullptr);
+            fcount.assign(count, 0);
+            fpool.assign(count, qlb_pool_view{nullptr, 0, nullptr, 0});
+            std::vector<std::string> errs(count);
+            std::atomic<uint32_t> next{0};
+            auto worker = [&] {
+                qlb_transpile_config tc;
+                qlb_transpile_config_default(&tc);
+                tc.enable_hw_awareness = 0;
+                tc.max_fusion_qubits = static_cast<int>(fuse_qubits);
+                for (uint32_t c; (c = next.fetch_add(1)) < count;) {
+                    if (qlb_transpile_gpu(programs_in[c], counts_in[c], &pools_in[c], num_qubits[c], &tc,
+                                          &fused.m[c]) != QLB_OK) {
+                        errs[c] = qlb_last_error();
+                        continue;
+                    }
+                    qlb_module_program(fused.m[c], &fprog[c], &fcount[c]);
+                    qlb_module_pool(fused.m[c], &fpool[c]);
+                }
+            };
+            unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+            nt = std::min<unsigned>(nt, count);
+            std::vector<std::thread> th;
+            for (unsigned i = 1; i < nt; ++i) th.emplace_back(worker);
+            worker();
+            for (auto& t : th) t.join();
+            for (uint32_t c = 0; c < count; ++c)
+                if (!errs[c].empty()) fail(QLB_ERR_INVALID_ARG, "circuit " + std::to_string(c) + " fusion: " + errs[c]);
+            programs = fprog.data();
+            counts = fcount.data();
+            pools = fpool.data();
+        }
         std::vector<int> choice(count, mode == QLB_MODE_TILED_TC ? 3 : 0);
         if (mode == -1) {
             const auto t0 = std::chrono::steady_clock::now();

@@ -158,6 +158,7 @@ Mat gate_matrix(const qlb_gate_instr& g, const Dag& d) {
 // Scatter-expansion of U (bit i <-> sub[i]) to the joint qubits `full`
 // (bit j <-> full[j]) (FusionMath::expand_matrix, middleware.hpp:241-312).
 Mat expand(const Mat& U, const std::vector<uint32_t>& sub, const std::vector<uint32_t>& full) {
+    if (sub == full) return U;           // the same qubits in the same order
     const uint32_t D = 1u << full.size();
     Mat M(D);
     std::vector<uint32_t> pos(sub.size());
@@ -171,9 +172,19 @@ Mat expand(const Mat& U, const std::vector<uint32_t>& sub, const std::vector<uin
         for (size_t i = 0; i < pos.size(); ++i) s |= ((x >> pos[i]) & 1u) << i;
         return s;
     };
-    for (uint32_t r = 0; r < D; ++r)
-        for (uint32_t c = 0; c < D; ++c)
-            if ((r & ~submask) == (c & ~submask)) M(r, c) = U(gather(r), gather(c));
+    // M(r, c) = U(gather(r), gather(c)) where r and c agree outside the
+    // sub-qubits: for each row, the columns are r's other bits | scat[s]
+    const uint32_t K = 1u << sub.size();
+    std::vector<uint32_t> scat(K);
+    for (uint32_t s = 0; s < K; ++s) {
+        uint32_t x = 0;
+        for (size_t i = 0; i < pos.size(); ++i) x |= ((s >> i) & 1u) << pos[i];
+        scat[s] = x;
+    }
+    for (uint32_t r = 0; r < D; ++r) {
+        const uint32_t rs = gather(r), base = r & ~submask;
+        for (uint32_t s = 0; s < K; ++s) M(r, base | scat[s]) = U(rs, s);
+    }
     return M;
 }
 
@@ -197,6 +208,32 @@ Mat fuse(const Mat& U1, const std::vector<uint32_t>& q1, const Mat& U2, const st
     for (uint32_t q : q2)
         if (std::find(out_q.begin(), out_q.end(), q) == out_q.end()) out_q.push_back(q);
     std::sort(out_q.begin(), out_q.end());
+    if (out_q == q1) {
+        // U2 acts inside U1's (sorted) qubits: mix U1's rows within each group
+        // of rows that differ only on U2's qubits (no expanded copy of U2)
+        const uint32_t D = U1.dim, K = U2.dim;
+        uint32_t submask = 0;
+        std::vector<uint32_t> scat(K, 0u);
+        for (size_t i = 0; i < q2.size(); ++i) {
+            const uint32_t p = static_cast<uint32_t>(std::find(q1.begin(), q1.end(), q2[i]) - q1.begin());
+            submask |= 1u << p;
+            for (uint32_t s = 0; s < K; ++s) scat[s] |= ((s >> i) & 1u) << p;
+        }
+        Mat M(D);
+        for (uint32_t b = 0; b < D; ++b) {
+            if (b & submask) continue;
+            for (uint32_t s = 0; s < K; ++s) {
+                cd* out = &M(b | scat[s], 0);
+                for (uint32_t t = 0; t < K; ++t) {
+                    const cd u = U2(s, t);
+                    if (u == cd(0.0, 0.0)) continue;
+                    const cd* in = &U1(b | scat[t], 0);
+                    for (uint32_t j = 0; j < D; ++j) out[j] += u * in[j];
+                }
+            }
+        }
+        return M;
+    }
     return matmul(expand(U2, q2, out_q), expand(U1, q1, out_q));
 }
 

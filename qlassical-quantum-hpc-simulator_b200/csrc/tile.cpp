@@ -1015,10 +1015,18 @@ private:
             for (const HostOp& h : acc.ops) emit_cuda_op(h);
         } else {
             std::vector<cd> U(32 * 32, cd(0.0, 0.0));
+            // A run that opens with a 5-qubit dense op (a fused block: its
+            // matrix order is the register order) starts from that matrix
+            // instead of simulating it on the 32 basis columns.
+            size_t first = 0;
+            if (acc.ops[0].kind == TOP_DENSE && acc.ops[0].k == 5 && acc.ops[0].cm == 0 && acc.ops[0].cmem == 0) {
+                std::copy(acc.ops[0].mat.begin(), acc.ops[0].mat.end(), U.begin());
+                first = 1;
+            }
             for (int c = 0; c < 32; ++c) {
                 cd col[32];
-                for (int r = 0; r < 32; ++r) col[r] = (r == c) ? cd(1.0, 0.0) : cd(0.0, 0.0);
-                for (const HostOp& h : acc.ops) apply_host(h, col);
+                for (int r = 0; r < 32; ++r) col[r] = first ? U[r * 32 + c] : ((r == c) ? cd(1.0, 0.0) : cd(0.0, 0.0));
+                for (size_t i = first; i < acc.ops.size(); ++i) apply_host(acc.ops[i], col);
                 for (int r = 0; r < 32; ++r) U[r * 32 + c] = col[r];
             }
             emit_tc_op(U, prog.ops.size() == entry_op_ ? entry_kperm_ : nullptr);

@@ -147,3 +147,21 @@ def test_engine_tile_low_option(mode, tile_low):
     assert oracle.max_abs_diff(st, e.state()) < 2e-5
     with pytest.raises(ValueError):
         e.set_option(q._lib.OPT_TILE_LOW, 7)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["tiled_tc", "auto"])
+def test_batch_fused_circuits_match_oracle(mode):
+    """fuse=5: each circuit is fused by the GPU middle end (blocks of up to 5
+    qubits) before planning; <Z> still match the oracle."""
+    mods = circuits.hea_batch(24, seed=17, n_min=10, n_max=16, d_min=4, d_max=10)
+    b = Batch(mods, mode, fuse=5)
+    b.run()
+    b.synchronize()
+    ez = b.expect_z()
+    for i, m in enumerate(mods):
+        want, _ = _oracle_ez(m)
+        assert np.max(np.abs(ez[i] - want)) < 5e-5, (i, m.num_qubits)
+    assert b.stats()["amp_updates"] == sum(m.gate_count() * 2 ** m.num_qubits for m in mods)
+    with pytest.raises(ValueError):
+        Batch(mods[:2], "tiled_tc", fuse=6)
