@@ -634,7 +634,8 @@ def batched_workload(q, args, rank=0, world=1, mode="auto"):
                    "circuits": len(mods), "mode": st["mode"], "fuse": f"GPU middle end in the batch, blocks of <= {fuse} qubits",
                    "rounds": st["rounds"], "passes": st["passes"],
                    "amp_updates_per_step": st["amp_updates"], "state_bytes": st["state_bytes"],
-                   "build_s": build_s,
+                   "build_s": build_s, "fuse_s": st.get("fuse_seconds"), "plan_s": st.get("plan_seconds"),
+                   "host_cpus": os.cpu_count(),
                    "l2": "4 GB of states, larger than the 126 MB L2"},
         "autotune": {"candidates": [q._lib.batch_tune_candidate(k) for k in range(q._lib.BATCH_TUNE_CANDIDATES)],
                      "method": "per size class: each candidate plans a sample of the class; CUDA events around "

@@ -355,6 +355,8 @@ typedef struct qlb_batch_info {
     uint32_t tune_classes;  /* mode -1: entries of tune[] in use */
     uint32_t pad;
     qlb_batch_tune_class tune[QLB_BATCH_TUNE_CLASSES];
+    double   fuse_seconds;  /* host time of the circuits' fusion (qlb_batch_create_ex) */
+    double   plan_seconds;  /* host time of the final planning, assembly and graph capture */
 } qlb_batch_info;
 
 /* Plans `count` circuits (program c: counts[c] instructions over pools[c],

@@ -127,6 +127,8 @@ class BatchInfo(ctypes.Structure):
         ("tune_classes", ctypes.c_uint32),
         ("pad", ctypes.c_uint32),
         ("tune", BatchTuneClass * BATCH_TUNE_CLASSES),
+        ("fuse_seconds", ctypes.c_double),
+        ("plan_seconds", ctypes.c_double),
     ]
 
 

@@ -95,6 +95,8 @@ class Batch:
             "amp_updates": info.amp_updates, "state_bytes": info.state_bytes,
             "autotune_ms": list(info.autotune_ms),
             "tune_seconds": info.tune_seconds,
+            "fuse_seconds": info.fuse_seconds,
+            "plan_seconds": info.plan_seconds,
             "tune": [{"num_qubits": t.num_qubits, "circuits": t.circuits, "sample": t.sample,
                       "best": _lib.batch_tune_candidate(t.best),
                       "ms": [float(x) for x in t.ms]}

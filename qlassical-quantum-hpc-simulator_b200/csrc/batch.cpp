@@ -71,7 +71,7 @@ struct qlb_batch {
     size_t o_states = 0, o_chunks = 0;
     std::unique_ptr<BatchProgram> prog;
     double autotune_ms[2] = {0.0, 0.0};
-    double tune_seconds = 0.0;
+    double tune_seconds = 0.0, fuse_seconds = 0.0, plan_seconds = 0.0;
     std::vector<qlb_batch_tune_class> tune;
     ~qlb_batch() {
         prog.reset();
@@ -133,11 +133,15 @@ std::vector<HostPlan> plan_jobs(const qlb_batch& b, const std::vector<PlanJob>& 
 std::unique_ptr<BatchProgram> assemble(qlb_batch& b, const std::vector<uint32_t>& members,
                                        std::vector<HostPlan>& plans, int mode) {
     const size_t C = members.size();
-    // merge
+    // merge the small arrays (passes, phases, ops: rebased); the matrix
+    // images, which tensor-core ops make large (16 KB each), go to the device
+    // straight from each plan
     auto P = std::make_unique<BatchProgram>();
     P->mode = mode;
     TileProgram all;
     std::vector<std::vector<uint32_t>> pass_ids(C);
+    std::vector<size_t> mat_at(C);   // float2 offset of each plan's matrices
+    size_t n_mats = 0;
     size_t max_passes = 0;
     for (size_t i = 0; i < C; ++i) {
         HostPlan& h = plans[i];
@@ -146,11 +150,12 @@ std::unique_ptr<BatchProgram> assemble(qlb_batch& b, const std::vector<uint32_t>
                 fail(QLB_ERR_INVALID_ARG, "circuit " + std::to_string(members[i]) +
                                               ": batched circuits may hold only gates (no MEASURE, no 6-qubit "
                                               "blocks, no physical GLOBAL_SWAP)");
-        if (all.mats.size() & 1) all.mats.push_back(make_float2(0.f, 0.f));
+        n_mats += n_mats & 1;        // each plan's matrices start on a 16-byte boundary
         const uint32_t pb = static_cast<uint32_t>(all.passes.size());
         const uint32_t phb = static_cast<uint32_t>(all.phases.size());
         const uint32_t ob = static_cast<uint32_t>(all.ops.size());
-        const uint32_t mb = static_cast<uint32_t>(all.mats.size());
+        const uint32_t mb = static_cast<uint32_t>(n_mats);
+        if (n_mats + h.prog.mats.size() > 0xFFFFFFFFull) fail(QLB_ERR_OOM, "batch matrix images exceed 32-bit offsets");
         for (TilePass p : h.prog.passes) {
             p.phase_begin += phb;
             p.phase_end += phb;
@@ -165,7 +170,8 @@ std::unique_ptr<BatchProgram> assemble(qlb_batch& b, const std::vector<uint32_t>
             op.data += mb;
             all.ops.push_back(op);
         }
-        all.mats.insert(all.mats.end(), h.prog.mats.begin(), h.prog.mats.end());
+        mat_at[i] = n_mats;
+        n_mats += h.prog.mats.size();
         for (const PlanStep& st : h.steps) pass_ids[i].push_back(pb + st.index);
         max_passes = std::max(max_passes, pass_ids[i].size());
         P->passes += pass_ids[i].size();
@@ -191,13 +197,14 @@ std::unique_ptr<BatchProgram> assemble(qlb_batch& b, const std::vector<uint32_t>
         P->tiles += R.tiles;
         P->rounds.push_back(R);
     }
+    // device layout: passes | phases | ops | work lists | tile maps | matrices
     P->o_pass = 0;
     P->o_phase = align256(all.passes.size() * sizeof(TilePass));
     P->o_ops = align256(P->o_phase + all.phases.size() * sizeof(TilePhase));
-    P->o_mat = align256(P->o_ops + all.ops.size() * sizeof(TileOp));
-    const size_t o_work = align256(P->o_mat + all.mats.size() * sizeof(float2));
+    const size_t o_work = align256(P->o_ops + all.ops.size() * sizeof(TileOp));
     const size_t o_tmap = align256(o_work + work.size() * sizeof(TileWork));
-    const size_t total = align256(o_tmap + tmap.size() * sizeof(uint32_t));
+    P->o_mat = align256(o_tmap + tmap.size() * sizeof(uint32_t));
+    const size_t total = align256(P->o_mat + n_mats * sizeof(float2));
     char* d = static_cast<char*>(P->dev.ensure(total));
     float2* base = static_cast<float2*>(b.state_buf.p);
     for (TileWork& w : work) {
@@ -208,11 +215,10 @@ std::unique_ptr<BatchProgram> assemble(qlb_batch& b, const std::vector<uint32_t>
         w.ops = reinterpret_cast<const TileOp*>(d + P->o_ops);
         w.mats = reinterpret_cast<const float2*>(d + P->o_mat);
     }
-    std::vector<char> h(total, 0);
+    std::vector<char> h(P->o_mat);
     std::memcpy(h.data() + P->o_pass, all.passes.data(), all.passes.size() * sizeof(TilePass));
     std::memcpy(h.data() + P->o_phase, all.phases.data(), all.phases.size() * sizeof(TilePhase));
     std::memcpy(h.data() + P->o_ops, all.ops.data(), all.ops.size() * sizeof(TileOp));
-    std::memcpy(h.data() + P->o_mat, all.mats.data(), all.mats.size() * sizeof(float2));
     std::memcpy(h.data() + o_work, work.data(), work.size() * sizeof(TileWork));
     std::memcpy(h.data() + o_tmap, tmap.data(), tmap.size() * sizeof(uint32_t));
     for (BatchRound& R : P->rounds) {
@@ -222,7 +228,12 @@ std::unique_ptr<BatchProgram> assemble(qlb_batch& b, const std::vector<uint32_t>
     // On the batch's stream: it does not synchronise with the legacy default
     // stream, and a cudaMemcpy from pageable memory may return before its DMA
     // has landed, so a launch on the batch's stream could read the program early.
-    check_cuda(cudaMemcpyAsync(d, h.data(), total, cudaMemcpyHostToDevice, b.stream), "batch program upload");
+    check_cuda(cudaMemcpyAsync(d, h.data(), h.size(), cudaMemcpyHostToDevice, b.stream), "batch program upload");
+    for (size_t i = 0; i < C; ++i)
+        if (!plans[i].prog.mats.empty())
+            check_cuda(cudaMemcpyAsync(d + P->o_mat + mat_at[i] * sizeof(float2), plans[i].prog.mats.data(),
+                                       plans[i].prog.mats.size() * sizeof(float2), cudaMemcpyHostToDevice, b.stream),
+                       "batch matrix upload");
     check_cuda(cudaStreamSynchronize(b.stream), "batch program upload");
     return P;
 }
@@ -497,6 +508,7 @@ int qlb_batch_create_ex(qlb_batch_t* out, uint32_t count, const qlb_gate_instr* 
         std::vector<uint64_t> fcount;
         std::vector<qlb_pool_view> fpool;
         if (fuse_qubits) {
+            const auto tf = std::chrono::steady_clock::now();
             if (fuse_qubits > 5) fail(QLB_ERR_INVALID_ARG, "batched fusion takes blocks of at most 5 qubits");
             fused.m.assign(count, nullptr);
             fprog.assign(count, nullptr);
@@ -530,6 +542,7 @@ int qlb_batch_create_ex(qlb_batch_t* out, uint32_t count, const qlb_gate_instr* 
             programs = fprog.data();
             counts = fcount.data();
             pools = fpool.data();
+            b->fuse_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tf).count();
         }
         std::vector<int> choice(count, mode == QLB_MODE_TILED_TC ? 3 : 0);
         if (mode == -1) {
@@ -537,8 +550,10 @@ int qlb_batch_create_ex(qlb_batch_t* out, uint32_t count, const qlb_gate_instr* 
             choice = autotune(*b, programs, counts, pools);
             b->tune_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         }
+        const auto tp = std::chrono::steady_clock::now();
         b->prog = build_program(*b, choice, programs, counts, pools);
         capture(*b, *b->prog);
+        b->plan_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tp).count();
         *out = b.release();
     });
 }
@@ -606,6 +621,8 @@ int qlb_batch_stats(qlb_batch_t b, qlb_batch_info* out) {
         out->autotune_ms[0] = b->autotune_ms[0];
         out->autotune_ms[1] = b->autotune_ms[1];
         out->tune_seconds = b->tune_seconds;
+        out->fuse_seconds = b->fuse_seconds;
+        out->plan_seconds = b->plan_seconds;
         out->tune_classes = static_cast<uint32_t>(b->tune.size());
         for (size_t i = 0; i < b->tune.size() && i < QLB_BATCH_TUNE_CLASSES; ++i) out->tune[i] = b->tune[i];
     });
