@@ -1148,7 +1148,9 @@ private:
         prog.ops.push_back(cont);
     }
 
-    void flush_pending(const PhaseBuild& pb, const int* local_of, Acc* acc, bool global) {
+    // Only the terms that share a qubit with `only` are emitted; the others
+    // commute with the gate that caused the flush and stay pending.
+    void flush_pending(const PhaseBuild& pb, const int* local_of, Acc* acc, bool global, uint64_t only = ~0ull) {
         cd R[32];
         for (cd& z : R) z = cd(1.0, 0.0);
         bool has_r = false;
@@ -1171,8 +1173,13 @@ private:
                 }
             T.push_back({cmem, p1, p0});
         };
+        std::vector<PTerm> stay;
         for (const PTerm& t : pend_) {
             if (is_one(t.p1) && is_one(t.p0)) continue;
+            if (!(t.mask & only)) {
+                stay.push_back(t);
+                continue;
+            }
             uint32_t cm;
             uint64_t cmem;
             split_mask(pb, local_of, t.mask, cm, cmem);
@@ -1203,8 +1210,9 @@ private:
                 Gs.push_back({cmem, cm, t.p1});
             }
         }
-        pend_.clear();
+        pend_.swap(stay);
         pend_qubits_ = 0;
+        for (const PTerm& t : pend_) pend_qubits_ |= t.mask;
         if (global) {
             const double g = wrap_angle(pass_global_);
             pass_global_ = 0.0;
@@ -1397,7 +1405,7 @@ private:
             }
             if (pend_qubits_ & m.targets) {
                 flush_rotations();
-                flush_pending(pb, local_of, tc ? &acc : nullptr, false);
+                flush_pending(pb, local_of, tc ? &acc : nullptr, false, m.targets);
             }
             for (HostOp& h : host_ops(pb, local_of, m)) {
                 if (!tc) {
