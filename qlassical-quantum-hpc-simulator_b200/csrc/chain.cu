@@ -22,7 +22,9 @@
 // twelfth warp issues the MMAs: a slot's 256 threads arrive on its "A ready"
 // barrier after writing A and B and go on to the other slot at once, so an
 // MMA issue that waits for the tensor pipe to drain the other slot's MMAs
-// stalls nobody.  HBM traffic: 16 B per amplitude per pass.
+// stalls nobody.  HBM traffic: 16 B per amplitude per pass.  The store of
+// a circuit's last pass also applies its deferred CZ-like sign terms (the
+// pass's post terms: a sign per amplitude from its memory index).
 //
 // The compute warps meet at one CTA barrier per tile (before the loaded
 // tile becomes A); otherwise only the MMA dependency orders them, so a warp
@@ -299,6 +301,8 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
 #pragma unroll
         for (int i = 0; i < 5; ++i)
             if ((lane >> i) & 1u) gl |= uint64_t{1} << P.tile_pos[1 + i];
+        uint64_t tilemem = 0;                          // memory bits of the tile qubits
+        for (int j = 0; j < kTileQubits; ++j) tilemem |= uint64_t{1} << P.tile_pos[j];
         bool ok = true;
         auto store = [&](uint64_t k) -> bool {
             const uint32_t b = static_cast<uint32_t>(k % kBufs);
@@ -311,12 +315,51 @@ k_tc_chain(TileWork w, uint64_t ntiles, int* __restrict__ err) {
             const uint4* src = reinterpret_cast<const uint4*>(bufs + b * kBufBytes);
             uint4* dst = reinterpret_cast<uint4*>(state);
             const uint32_t fl = fold4(2u * lane);
+            const uint32_t np = P.post_n;
+            if (np == 0) {
 #pragma unroll 6
-            for (uint32_t c = pw; c < 128; c += kProducerWarps) {
-                const uint32_t f = fl ^ fold4(64u * c);
-                uint4 v = src[(lane + 32u * c) ^ (f >> 1)];
-                if (f & 1u) v = make_uint4(v.z, v.w, v.x, v.y);
-                dst[(g0 | rowoff[c]) >> 1] = v;     // amplitudes g, g + 1 (g even)
+                for (uint32_t c = pw; c < 128; c += kProducerWarps) {
+                    const uint32_t f = fl ^ fold4(64u * c);
+                    uint4 v = src[(lane + 32u * c) ^ (f >> 1)];
+                    if (f & 1u) v = make_uint4(v.z, v.w, v.x, v.y);
+                    dst[(g0 | rowoff[c]) >> 1] = v;     // amplitudes g, g + 1 (g even)
+                }
+            } else {
+                // the circuit's last pass: its sign terms (CZ-like) flip sign
+                // bits on the way out.  Piece i = lane + 32 c holds tile-local
+                // amplitudes L = 2 lane + 64 c (+ 1): a term whose out-of-tile
+                // and lane bits this thread's tile has fires for the pieces
+                // whose row and bit 0 hold the rest of its tile-local mask.
+                uint32_t need[kPostMax], s0m[kPostMax];
+#pragma unroll
+                for (uint32_t i = 0; i < kPostMax; ++i) {
+                    need[i] = 0xFFFFFFFFu;      // never met: L < 2^13
+                    s0m[i] = 0u;
+                    if (i < np) {
+                        const uint32_t* r = reinterpret_cast<const uint32_t*>(w.mats + P.post_data + 4u * i);
+                        const uint64_t mask = r[0] | (uint64_t{r[1]} << 32);
+                        const uint32_t tl = r[6];
+                        if (((mask & ~tilemem) & ~g0) == 0 && ((tl & 0x3Eu) & ~(2u * lane)) == 0) {
+                            need[i] = tl & 0x1FC1u;
+                            s0m[i] = (tl & 1u) ? 0u : 0x80000000u;
+                        }
+                    }
+                }
+#pragma unroll 6
+                for (uint32_t c = pw; c < 128; c += kProducerWarps) {
+                    const uint32_t f = fl ^ fold4(64u * c);
+                    uint4 v = src[(lane + 32u * c) ^ (f >> 1)];
+                    if (f & 1u) v = make_uint4(v.z, v.w, v.x, v.y);
+                    const uint32_t l1 = 64u * c + 1u;
+                    uint32_t s0 = 0u, s1 = 0u;
+#pragma unroll
+                    for (uint32_t i = 0; i < kPostMax; ++i) {
+                        const uint32_t hit = (l1 & need[i]) == need[i] ? 0x80000000u : 0u;
+                        s1 ^= hit;
+                        s0 ^= hit & s0m[i];
+                    }
+                    dst[(g0 | rowoff[c]) >> 1] = make_uint4(v.x ^ s0, v.y ^ s0, v.z ^ s1, v.w ^ s1);
+                }
             }
             return true;
         };

@@ -647,7 +647,19 @@ private:
         P.phase_end = static_cast<uint32_t>(prog.phases.size());
         P.n_low = 0;
         while (P.n_low < kTileQubits && P.tile_pos[P.n_low] == P.n_low) ++P.n_low;
-        if (chain_form(P)) {
+        const bool chain = chain_form(P);
+        if (post_taken_) {
+            if (chain) {
+                emit_post(P);
+            } else {
+                for (const PTerm& x : post_terms_) add_pending(x.mask, x.p1, x.p0);
+                flush_pending(phases.back(), local_of, nullptr, true);
+                prog.phases.back().op_end = static_cast<uint32_t>(prog.ops.size());
+            }
+            post_terms_.clear();
+            post_taken_ = false;
+        }
+        if (chain) {
             pass_features_ |= kPassChain;
             stats.chain_passes += 1;
         }
@@ -1010,6 +1022,7 @@ private:
     // kernel on it goes to the tensor cores whatever its cost (the phase is
     // then a single tensor-core op, which a chain pass is made of).
     void flush(Acc& acc, bool whole_phase = false) {
+        for (PTerm& t : pend_) t.after_acc = false;     // every pending term now follows the run
         if (acc.ops.empty()) return;
         if (acc.cost < e_.tc_min_cost && !(whole_phase && e_.tc_chain)) {   // cheaper as CUDA-core ops
             for (const HostOp& h : acc.ops) emit_cuda_op(h);
@@ -1054,18 +1067,20 @@ private:
     struct PTerm {
         uint64_t mask;
         cd p1, p0;
+        bool after_acc = false;   // must follow the accumulator's current contents
     };
     std::vector<PTerm> pend_;
     uint64_t pend_qubits_ = 0;
 
-    void add_pending(uint64_t mask, cd p1, cd p0) {
+    void add_pending(uint64_t mask, cd p1, cd p0, bool after_acc = false) {
         for (PTerm& t : pend_)
             if (t.mask == mask) {
                 t.p1 *= p1;
                 t.p0 *= p0;
+                t.after_acc = t.after_acc || after_acc;
                 return;
             }
-        pend_.push_back({mask, p1, p0});
+        pend_.push_back({mask, p1, p0, after_acc});
         pend_qubits_ |= mask;
     }
 
@@ -1173,6 +1188,14 @@ private:
                 }
             T.push_back({cmem, p1, p0});
         };
+        // terms that came after a gate of the accumulated run on their
+        // register bits are emitted after the run
+        if (acc)
+            for (const PTerm& t : pend_)
+                if (t.after_acc && (t.mask & only)) {
+                    flush(*acc);
+                    break;
+                }
         std::vector<PTerm> stay;
         for (const PTerm& t : pend_) {
             if (is_one(t.p1) && is_one(t.p0)) continue;
@@ -1397,7 +1420,17 @@ private:
                             acc.ops.push_back(std::move(h));
                             continue;
                         }
-                        if (cm & acc.touched) flush(acc);
+                        // a term on register bits the run acts on must follow
+                        // the run: with the chain kernel on it is marked so (a
+                        // later flush emits it after the run, a post term
+                        // follows everything), else the run is emitted now
+                        if (cm & acc.touched) {
+                            if (e_.tc_chain) {
+                                add_pending(mask, p1, p0, true);
+                                continue;
+                            }
+                            flush(acc);
+                        }
                     }
                     add_pending(mask, p1, p0);
                 }
@@ -1439,8 +1472,78 @@ private:
             }
         }
         flush_rotations();
-        if (last_phase) flush_pending(pb, local_of, tc ? &acc : nullptr, true);
+        if (last_phase && !(tc && e_.tc_chain && take_post(pb, local_of, acc)))
+            flush_pending(pb, local_of, tc ? &acc : nullptr, true);
         if (tc) flush(acc, prog.ops.size() == phase_ops_begin_);
+    }
+
+    // ---- post terms --------------------------------------------------------
+    // At the end of a final pass in chain mode the deferred diagonal terms
+    // leave the last phase, so that its tensor-core op stays alone in it: sign
+    // terms (a CZ-like -1 where every mask bit is set, on any memory qubits)
+    // become post terms, which the chain kernel applies as it stores the tile
+    // (TilePass::post_*); register-only terms and the global phase join the
+    // accumulated run.  If the pass does not run on the chain kernel after
+    // all, the sign terms return as a TOP_DIAG op at the end of the last
+    // phase (they commute with everything the phase applies after them).
+    std::vector<PTerm> post_terms_;
+    bool post_taken_ = false;
+
+    bool take_post(const PhaseBuild& pb, const int* local_of, Acc& acc) {
+        std::vector<PTerm> sign, reg;
+        for (const PTerm& x : pend_) {
+            if (is_one(x.p1) && is_one(x.p0)) continue;
+            if (std::abs(x.p1 + cd(1.0, 0.0)) < 1e-12 && is_one(x.p0)) {
+                sign.push_back(x);
+                continue;
+            }
+            uint32_t cm;
+            uint64_t cmem;
+            split_mask(pb, local_of, x.mask, cm, cmem);
+            if (cmem != 0) return false;
+            reg.push_back(x);
+        }
+        if (sign.empty() || sign.size() > kPostMax) return false;
+        for (const PTerm& x : reg) {
+            uint32_t cm;
+            uint64_t cmem;
+            split_mask(pb, local_of, x.mask, cm, cmem);
+            HostOp h = diag_host_op(cm, x.p1, x.p0);
+            acc.cost += h.cost;
+            acc.ops.push_back(std::move(h));
+        }
+        const double g = wrap_angle(pass_global_);
+        if (g != 0.0) {
+            HostOp h = diag_host_op(0u, std::polar(1.0, g), cd(1.0, 0.0));
+            acc.cost += h.cost;
+            acc.ops.push_back(std::move(h));
+        }
+        post_terms_.swap(sign);
+        post_taken_ = true;
+        pend_.clear();
+        pend_qubits_ = 0;
+        pass_global_ = 0.0;
+        return true;
+    }
+
+    void emit_post(TilePass& P) {
+        const std::vector<PTerm>& t = post_terms_;
+        P.post_n = static_cast<uint32_t>(t.size());
+        P.post_data = 0;
+        if (t.empty()) return;
+        if (prog.mats.size() & 1) prog.mats.push_back(make_float2(0.f, 0.f));
+        P.post_data = static_cast<uint32_t>(prog.mats.size());
+        for (const PTerm& x : t) {
+            float2 w[4];
+            std::memcpy(&w[0], &x.mask, 8);
+            w[1] = make_float2(static_cast<float>(x.p1.real()), static_cast<float>(x.p1.imag()));
+            w[2] = make_float2(static_cast<float>(x.p0.real()), static_cast<float>(x.p0.imag()));
+            uint32_t tl[2] = {0u, 0u};
+            for (int j = 0; j < kTileQubits; ++j)
+                if (x.mask & bitm(P.tile_pos[j])) tl[0] |= 1u << j;
+            std::memcpy(&w[3], tl, 8);
+            for (const float2& f : w) prog.mats.push_back(f);
+        }
     }
 };
 
@@ -1545,6 +1648,10 @@ std::string describe_plan_json(const PlanConfig& cfg, const qlb_gate_instr* prog
         u(P.n_low);
         out += ",\"features\":";
         u(P.features);
+        out += ",\"post_data\":";
+        u(P.post_data);
+        out += ",\"post_n\":";
+        u(P.post_n);
         out += ",\"phases\":[";
         for (uint32_t ph = P.phase_begin; ph < P.phase_end; ++ph) {
             const TilePhase& T = pl.prog.phases[ph];

@@ -143,7 +143,16 @@ struct TilePass {
     uint8_t features;                 // kernel features the pass needs (kPass* bits)
     uint8_t out_mem[40];              // non-tile memory qubits, ascending
     uint32_t phase_begin, phase_end;
+    // Chain passes only: post_n (<= kPostMax) sign terms applied to every
+    // amplitude as the tile is stored, 32 B each at float2 offset post_data of
+    // the matrix buffer: {u64 memory mask, float2 p1 = -1, float2 p0 = 1,
+    // u32 the mask's tile-local bits, u32 0} -- an amplitude whose memory
+    // index has every mask bit set changes sign.
+    uint32_t post_data, post_n;
+    uint32_t pad[2];
 };
+static_assert(sizeof(TilePass) == 80, "TilePass layout (16-byte multiple)");
+constexpr uint32_t kPostMax = 4;
 
 // Device program of one execute(): all passes, phases, ops, matrices.
 struct TileProgram {

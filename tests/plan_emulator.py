@@ -47,6 +47,7 @@ def emulate(plan, init=None):
             continue
         if kind == STEP_PASS:
             P = plan["passes"][step["index"]]
+            assert P.get("post_n", 0) == 0, "post terms on a pass the general tile kernel runs"
             tp = P["tile_pos"]
             for ph in P["phases"]:
                 mq = [tp[r] for r in ph["reg_pos"]]
@@ -272,3 +273,22 @@ def emulate_chain_pass(plan, P, st, n):
         L = phases[last]
         g = base | _bits_or(t, [tp[p] for p in L["thr_pos"]]) | _bits_or(r, [tp[p] for p in L["reg_pos"]])
         st[g] = v
+    apply_post_terms(plan, P, st, n)
+
+
+def post_terms(plan, P):
+    """The pass's post terms (TilePass::post_*): (memory mask, p1, p0) from
+    32-byte records {u64 mask, float2 p1, float2 p0, pad} of the matrix buffer."""
+    words = np.array(plan["mats"], dtype=np.uint32)
+    out = []
+    for i in range(P.get("post_n", 0)):
+        w = words[2 * P["post_data"] + 8 * i: 2 * P["post_data"] + 8 * i + 8]
+        f = w[2:6].view(np.float32).astype(np.float64)
+        out.append((int(w[0]) | (int(w[1]) << 32), f[0] + 1j * f[1], f[2] + 1j * f[3]))
+    return out
+
+
+def apply_post_terms(plan, P, st, n):
+    idx = np.arange(1 << n, dtype=np.int64)
+    for mask, p1, p0 in post_terms(plan, P):
+        st *= np.where((idx & mask) == mask, p1, p0)

@@ -79,3 +79,23 @@ def test_chain_single_op_passes_and_small_grid():
         got, st = run(m, True, init=init)
         assert st["chain_passes"] >= 1 and st["tc_ops"] >= 1, st
         check(ref, got)
+
+
+@pytest.mark.parametrize("n", [15, 17])
+@pytest.mark.parametrize("signs_only", [True, False])
+def test_chain_post_terms_of_the_last_pass(n, signs_only):
+    """CZs that end the circuit (across out-of-tile and in-tile qubits) are
+    applied by the chain kernel's producers as sign flips while the last
+    pass stores each tile; with an RZ and a CP among them they stay a
+    diagonal op of the general kernel."""
+    from test_planner_emulated import _ends_with_diagonals
+    from qlassical_b200.engine import describe_plan
+    m = _ends_with_diagonals(n, n, signs_only)
+    plan = describe_plan(m, n, "tiled_tc")
+    assert (plan["passes"][-1]["post_n"] >= 2) == signs_only
+    init = zoo.random_state(n, 4)
+    ref, _ = oracle.run_oracle(m, init=init)
+    on, _ = run(m, True, init=init)
+    off, _ = run(m, False, init=init)
+    check(ref, on)
+    check(ref, off)

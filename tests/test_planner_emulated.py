@@ -152,6 +152,87 @@ def test_chain_passes_of_the_fused_rotation_circuit(n, depth):
     assert oracle.infidelity(want, got) < 1e-6
 
 
+def _ends_with_diagonals(n, seed, signs_only=True):
+    """5-qubit unitaries on tile qubits, then diagonal gates that no later
+    gate targets: CZs across out-of-tile and in-tile qubits (sign terms);
+    with signs_only False also an RZ and a CP on out-of-tile qubits."""
+    import qlassical_b200 as q
+    rng = np.random.default_rng(seed)
+    qc = q.QuantumCircuit(n)
+    for _ in range(4):
+        qc.unitary([int(x) for x in rng.permutation(13)[:5]], zoo.random_unitary(5, rng))
+    qc.cz(n - 3, n - 1)
+    qc.cz(3, n - 2)
+    qc.cz(0, 1)
+    if not signs_only:
+        qc.rz(n - 2, 0.7)
+        qc.cp(3, n - 1, 0.4)
+    qc.cz(2, 5)
+    return qc.release()
+
+
+@pytest.mark.parametrize("n", [15, 17])
+def test_post_terms_of_the_last_chain_pass(n):
+    """CZs still deferred at the end of the circuit leave the last pass's
+    phases (which stay chain phases) and become its post terms, applied as
+    sign flips as the chain kernel stores the tile; with the chain kernel
+    off, or with a non-sign term among them (RZ, CP on out-of-tile qubits),
+    they are a diagonal op in the last phase instead."""
+    m = _ends_with_diagonals(n, n)
+    init = zoo.random_state(n, 4)
+    plan = check(m, "tiled_tc", init=init)
+    P = plan["passes"][-1]
+    assert P["features"] & 32 and P["post_n"] >= 2, (P["features"], P["post_n"])
+    off = check(m, "tiled_tc", init=init, tc_chain=False)
+    assert all(Q["post_n"] == 0 for Q in off["passes"])
+    mixed = check(_ends_with_diagonals(n, n, signs_only=False), "tiled_tc", init=init)
+    assert all(Q["post_n"] == 0 for Q in mixed["passes"])
+    # the fused rotation circuit's last pass carries its trailing CZs this way
+    from qlassical_b200.middleware import Middleware, TranspilerConfig
+    f = Middleware().transpile(circuits.random_rot_cz(16, 8, seed=1), config=TranspilerConfig(max_fusion_qubits=5))
+    plan = check(f, "tiled_tc")
+    assert plan["passes"][-1]["post_n"] >= 1
+
+
+def test_post_sign_terms_as_the_producers_apply_them():
+    """The chain kernel's producers apply a sign term to piece i = lane +
+    32 c (tile-local amplitudes L = 2 lane + 64 c and L + 1) of a tile from
+    the term's tile-local mask (record word 6): live when the tile's
+    out-of-tile bits and the lane's bits hold the mask's, then firing where
+    64 c + 1 holds the rest (amplitude L + 1) and, if the mask has no bit 0,
+    for amplitude L too.  Compared with the memory-index rule on every piece
+    of several tiles."""
+    from plan_emulator import post_terms
+    n = 17
+    m = _ends_with_diagonals(n, n)
+    plan = describe_plan(m, n, "tiled_tc")
+    P = plan["passes"][-1]
+    assert 1 <= P["post_n"] <= 4
+    words = np.array(plan["mats"], dtype=np.uint32)
+    tp = P["tile_pos"]
+    tilemem = sum(1 << q for q in tp)
+    out_mem = [q for q in range(n) if not (tilemem >> q) & 1]
+    lane = np.arange(32)[:, None]
+    c = np.arange(128)[None, :]
+    L0 = 2 * lane + 64 * c                                       # (32, 128)
+    to_mem = lambda L: sum(((L >> j) & 1) << tp[j] for j in range(13))
+    for i, (mask, p1, p0) in enumerate(post_terms(plan, P)):
+        assert abs(p1 + 1) < 1e-6 and abs(p0 - 1) < 1e-6
+        tl = int(words[2 * P["post_data"] + 8 * i + 6])
+        assert to_mem(tl) == mask & tilemem
+        for tile in range(1 << len(out_mem)):
+            base = sum(((tile >> j) & 1) << q for j, q in enumerate(out_mem))
+            gl = to_mem(2 * lane)
+            live = ((mask & ~tilemem) & ~base) == 0
+            live = live & (((tl & 0x3E) & ~(2 * lane)) == 0)      # (32, 1)
+            need = tl & 0x1FC1
+            hit1 = live & (((64 * c + 1) & need) == need)
+            hit0 = hit1 & ((tl & 1) == 0)
+            g = base | to_mem(L0)
+            assert np.array_equal(hit0, (g & mask) == mask)
+            assert np.array_equal(hit1, ((g | 1) & mask) == mask)
+
+
 def test_chain_producer_piece_addressing():
     """The chain kernel's producer warps move 16-byte pieces: piece i =
     lane + 32 c of a tile holds tile-local amplitudes 2 i, 2 i + 1, at
