@@ -1438,7 +1438,10 @@ private:
             }
             if (pend_qubits_ & m.targets) {
                 flush_rotations();
-                flush_pending(pb, local_of, tc ? &acc : nullptr, false, m.targets);
+                // tensor-core mode: only the terms on the gate's targets, so
+                // the others can still join a later run or the post terms;
+                // CUDA-core mode: all of them, in one op
+                flush_pending(pb, local_of, tc ? &acc : nullptr, false, tc ? m.targets : ~0ull);
             }
             for (HostOp& h : host_ops(pb, local_of, m)) {
                 if (!tc) {
