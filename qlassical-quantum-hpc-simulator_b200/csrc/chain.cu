@@ -14,12 +14,12 @@
 // tensor-memory columns and its own B staging): while slot 0's MMAs run,
 // the 256 compute threads convert slot 1's tile, and the other way round.
 // Slot 1 starts half a tile behind slot 0, so its buffer's next load has
-// time to land.  Three producer warps move the tiles between HBM and three
+// time to land.  Four producer warps move the tiles between HBM and three
 // 64 KB buffers: 16-byte cp.async pieces (TMA bulk copies for runs of
 // >= 4 KB) into a buffer, and, after the last op, the result that the
 // compute warps staged in the buffer (bank-swizzled tile order) back to
 // HBM with 16-byte stores; then the buffer takes the tile three ahead.  A
-// twelfth warp issues the MMAs: a slot's 256 threads arrive on its "A ready"
+// thirteenth warp issues the MMAs: a slot's 256 threads arrive on its "A ready"
 // barrier after writing A and B and go on to the other slot at once, so an
 // MMA issue that waits for the tensor pipe to drain the other slot's MMAs
 // stalls nobody.  HBM traffic: 16 B per amplitude per pass.  The store of
@@ -45,12 +45,13 @@ namespace {
 using namespace ptx;
 
 constexpr int kCompute = 256;                     // thread t converts A / D row t
-constexpr int kProducerWarps = 3;                // warps 8..10: HBM <-> buffers
+constexpr int kProducerWarps = 4;                // warps 8..11: HBM <-> buffers
 constexpr int kProducers = 32 * kProducerWarps;
-constexpr int kMmaThread = kCompute + kProducers; // warp 11, first lane: MMA issue
-// 384 threads, up to 168 registers a thread.  (Measured on the fused
-// 30-qubit circuit: seven producer warps, at 128 registers, or two compute
-// threads per row, at 80, ran no faster -- the copies keep up with three.)
+constexpr int kMmaThread = kCompute + kProducers; // warp 12, first lane: MMA issue
+// 416 threads, 128 registers a thread (no spills).  Measured on the fused
+// 30-qubit circuit: four producer warps 0.7 % faster than three (at 143
+// registers), five 0.4 % slower than three; seven, or two compute threads
+// per row (at 80 registers), ran no faster.
 constexpr int kThreads = kCompute + kProducers + 32;
 constexpr uint32_t kTile = 1u << kTileQubits;
 constexpr uint32_t kBufBytes = kTile * 8u;        // 64 KB: the tile (fp32) or its A operand (bf16 hi | lo)

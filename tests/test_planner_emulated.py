@@ -239,17 +239,17 @@ def test_chain_producer_piece_addressing():
     memory index (lane's bits 1..5 -> tile qubits 1..5) | rowoff[c] (c's
     bits -> tile qubits 6..12) (chain.cu).  Every piece of the 64 KB buffer
     is covered exactly once, from the memory index its tile-local index
-    maps to; producer warp w takes the rows c = w, w + 3, ..."""
+    maps to; producer warp w of W takes the rows c = w, w + W, ..."""
     rng = np.random.default_rng(3)
-    for _ in range(4):
+    for warps in (3, 4, 4, 5):
         tp = [0, 1, 2] + sorted(int(x) for x in rng.choice(np.arange(3, 30), 10, replace=False))
         mem_of = lambda l: sum(1 << tp[j] for j in range(13) if (l >> j) & 1)   # noqa: E731
         rowoff = [sum(1 << tp[6 + i] for i in range(7) if (c >> i) & 1) for c in range(128)]
         seen = {}
-        for pw in range(3):
+        for pw in range(warps):
             for lane in range(32):
                 gl = sum(1 << tp[1 + i] for i in range(5) if (lane >> i) & 1)
-                for c in range(pw, 128, 3):
+                for c in range(pw, 128, warps):
                     d = 16 * lane + 512 * c
                     assert d not in seen
                     seen[d] = gl | rowoff[c]
