@@ -194,6 +194,28 @@ def test_post_terms_of_the_last_chain_pass(n):
     assert plan["passes"][-1]["post_n"] >= 1
 
 
+@pytest.mark.parametrize("chain", [True, False])
+def test_diagonal_term_after_a_tensor_core_run(chain):
+    """A CP between a register qubit of the run being fused for the tensor
+    cores and a qubit outside it, followed by more gates on the run's qubits
+    and then a gate on the CP's register qubit: the term must land after the
+    run (chain mode marks it and flushes the run first; otherwise the run
+    is emitted when the term arrives), and before that last gate."""
+    import qlassical_b200 as q
+    rng = np.random.default_rng(21)
+    n = 15
+    qc = q.QuantumCircuit(n)
+    qc.unitary([0, 1, 2, 3, 4], zoo.random_unitary(5, rng))
+    qc.cp(2, 14, 0.9)
+    qc.ry(3, 0.4)
+    qc.unitary([1, 3], zoo.random_unitary(2, rng))
+    qc.h(2)
+    qc.cz(4, 13)
+    qc.rx(4, -0.3)
+    m = qc.release()
+    check(m, "tiled_tc", init=zoo.random_state(n, 6), tc_chain=chain)
+
+
 def test_post_sign_terms_as_the_producers_apply_them():
     """The chain kernel's producers apply a sign term to piece i = lane +
     32 c (tile-local amplitudes L = 2 lane + 64 c and L + 1) of a tile from
