@@ -48,7 +48,9 @@ constexpr int kCompute = 256;                     // thread t converts A / D row
 constexpr int kProducerWarps = 4;                // warps 8..11: HBM <-> buffers
 constexpr int kProducers = 32 * kProducerWarps;
 constexpr int kMmaThread = kCompute + kProducers; // warp 12, first lane: MMA issue
-// 416 threads, 128 registers a thread (no spills).  Measured on the fused
+// 416 threads, 128 registers a thread (no spills; 13 warps put four on one
+// SM sub-partition, whose 16,384 registers cap a thread at 128 -- a build
+// at 137 was refused at launch).  Measured on the fused
 // 30-qubit circuit: four producer warps 0.7 % faster than three (at 143
 // registers), five 0.4 % slower than three; seven, or two compute threads
 // per row (at 80 registers), ran no faster.
